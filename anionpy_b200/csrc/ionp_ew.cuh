@@ -1,0 +1,262 @@
+// Element-wise kernels (ufunc __call__ hot path).
+//
+//  k_bin_contig / k_un_contig : operands contiguous (or 0-d broadcast) in the
+//      loop dtype, 16-byte aligned: 128-bit vector loads/stores, unrolled so
+//      each thread keeps several independent loads in flight, streaming cache
+//      hints (data is touched once).
+//  k_bin_nd / k_un_nd : up to 4 merged dims with arbitrary element strides
+//      (broadcast axes have stride 0), cast-on-load from any operand dtype,
+//      cast-on-store to the out= dtype, optional where= mask. Long inner rows
+//      are walked in coalesced row tiles; short rows use a flat index.
+// The per-element arithmetic is BinOp/UnOp from ionp_scalar.cuh / ionp_math.cuh.
+#pragma once
+#include "ionp_scalar.cuh"
+#include "ionp_math.cuh"
+#include "ionp_internal.h"
+
+namespace ionp {
+
+constexpr int EW_THREADS = 256;
+
+__device__ __forceinline__ void flush_flags(uint32_t bits, uint32_t* flags) {
+    bits = __reduce_or_sync(0xffffffffu, bits);
+    if (bits && (threadIdx.x & 31) == 0) atomicOr(flags, bits);
+}
+
+template <class T> struct Vec16 {
+    static constexpr int N = 16 / (int)sizeof(T);
+    T v[N];
+};
+template <class T> __device__ __forceinline__ Vec16<T> ldv(const T* p, int64_t i) {
+    Vec16<T> r;
+    uint4 u = __ldcs(reinterpret_cast<const uint4*>(p) + i);
+    memcpy(&r, &u, 16);
+    return r;
+}
+// store N results of type R (N*sizeof(R) bytes, naturally aligned)
+template <class R, int N> __device__ __forceinline__ void stv(R* p, int64_t i, const R (&r)[N]) {
+    constexpr int B = N * (int)sizeof(R);
+    if constexpr (B == 16) { uint4 u; memcpy(&u, r, 16); __stcs(reinterpret_cast<uint4*>(p) + i, u); }
+    else if constexpr (B == 8) { uint2 u; memcpy(&u, r, 8); __stcs(reinterpret_cast<uint2*>(p) + i, u); }
+    else if constexpr (B == 4) { unsigned u; memcpy(&u, r, 4); __stcs(reinterpret_cast<unsigned*>(p) + i, u); }
+    else if constexpr (B == 2) { unsigned short u; memcpy(&u, r, 2); reinterpret_cast<unsigned short*>(p)[i] = u; }
+    else { for (int k = 0; k < N; ++k) p[i * N + k] = r[k]; }
+}
+
+// ---------------------------------------------------------------------------
+// binary
+// ---------------------------------------------------------------------------
+template <int OP, int CD, bool FPE>
+__global__ void __launch_bounds__(EW_THREADS)
+k_bin_contig(const typename DT<CD>::T* __restrict__ a, const typename DT<CD>::T* __restrict__ b,
+             typename BinOp<OP, CD>::R* __restrict__ o, int64_t n, int a_sc, int b_sc, uint32_t* flags) {
+    typedef typename DT<CD>::T T;
+    typedef typename BinOp<OP, CD>::R R;
+    constexpr int N = Vec16<T>::N;
+    constexpr int U = 2;  // vectors per thread per iteration
+    uint32_t bits = 0;
+    const T a0 = a[0], b0 = b[0];
+    const int64_t nvec = n / N;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    for (; v + (U - 1) * stride < nvec; v += U * stride) {
+        Vec16<T> xa[U], xb[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            if (!a_sc) xa[u] = ldv(a, v + u * stride); else for (int k = 0; k < N; ++k) xa[u].v[k] = a0;
+            if (!b_sc) xb[u] = ldv(b, v + u * stride); else for (int k = 0; k < N; ++k) xb[u].v[k] = b0;
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            R r[N];
+#pragma unroll
+            for (int k = 0; k < N; ++k) {
+                r[k] = BinOp<OP, CD>::apply(xa[u].v[k], xb[u].v[k]);
+                if constexpr (FPE) bits |= fpe_bits<OP, CD>(xa[u].v[k], xb[u].v[k], r[k]);
+            }
+            stv<R, N>(o, v + u * stride, r);
+        }
+    }
+    for (; v < nvec; v += stride) {
+        Vec16<T> xa, xb;
+        if (!a_sc) xa = ldv(a, v); else for (int k = 0; k < N; ++k) xa.v[k] = a0;
+        if (!b_sc) xb = ldv(b, v); else for (int k = 0; k < N; ++k) xb.v[k] = b0;
+        R r[N];
+#pragma unroll
+        for (int k = 0; k < N; ++k) {
+            r[k] = BinOp<OP, CD>::apply(xa.v[k], xb.v[k]);
+            if constexpr (FPE) bits |= fpe_bits<OP, CD>(xa.v[k], xb.v[k], r[k]);
+        }
+        stv<R, N>(o, v, r);
+    }
+    // tail
+    for (int64_t i = nvec * N + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+        T x = a_sc ? a0 : a[i], y = b_sc ? b0 : b[i];
+        R r = BinOp<OP, CD>::apply(x, y);
+        if constexpr (FPE) bits |= fpe_bits<OP, CD>(x, y, r);
+        o[i] = r;
+    }
+    if constexpr (FPE) flush_flags(bits, flags);
+}
+
+// Offsets of flat index i over the merged dims (C order, last dim fastest).
+struct Offs { int64_t a, b, o, m; };
+__device__ __forceinline__ Offs unravel(const EwDesc& d, int64_t i, int nd_from_end) {
+    Offs r = {0, 0, 0, 0};
+    for (int k = d.nd - 1 - nd_from_end; k >= 0; --k) {
+        int64_t s = d.shape[k];
+        int64_t q = i / s;
+        int64_t id = i - q * s;
+        i = q;
+        r.a += id * d.a.st[k]; r.b += id * d.b.st[k]; r.o += id * d.so[k]; r.m += id * d.m.st[k];
+    }
+    return r;
+}
+
+template <int OP, int CD, bool FPE, bool SAME>
+__global__ void __launch_bounds__(EW_THREADS)
+k_bin_nd(EwDesc d, uint32_t* flags) {
+    typedef typename DT<CD>::T T;
+    typedef BinOp<OP, CD> Op;
+    typedef typename Op::R R;
+    uint32_t bits = 0;
+    const int nd = d.nd;
+    const int64_t inner = d.shape[nd - 1];
+    const int64_t sa = d.a.st[nd - 1], sb = d.b.st[nd - 1], so = d.so[nd - 1], sm = d.m.st[nd - 1];
+    const bool has_m = d.m.p != nullptr;
+    auto one = [&](int64_t oa, int64_t ob, int64_t oo, int64_t om) {
+        T x, y;
+        if constexpr (SAME) { x = ((const T*)d.a.p)[oa]; y = ((const T*)d.b.p)[ob]; }
+        else { x = load_cast<CD>(d.a.p, oa, d.a.dt); y = load_cast<CD>(d.b.p, ob, d.b.dt); }
+        R r = Op::apply(x, y);
+        if constexpr (FPE) bits |= fpe_bits<OP, CD>(x, y, r);
+        if (has_m && !((const uint8_t*)d.m.p)[om]) return;
+        if constexpr (SAME) ((R*)d.o)[oo] = r;
+        else store_cast<Op::OUT_DT>(d.o, oo, d.odt, r);
+    };
+    if (inner >= 64) {
+        constexpr int ILP = 4;
+        const int64_t tile = (int64_t)blockDim.x * ILP;
+        const int64_t tpr = (inner + tile - 1) / tile;
+        const int64_t rows = d.n / inner;
+        const int64_t ntiles = rows * tpr;
+        for (int64_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
+            int64_t row = t / tpr, cb = t - row * tpr;
+            Offs base = unravel(d, row, 1);
+            int64_t c0 = cb * tile + threadIdx.x;
+#pragma unroll
+            for (int u = 0; u < ILP; ++u) {
+                int64_t c = c0 + u * blockDim.x;
+                if (c < inner) one(base.a + c * sa, base.b + c * sb, base.o + c * so, base.m + c * sm);
+            }
+        }
+    } else {
+        const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+        for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < d.n; i += stride) {
+            Offs f = unravel(d, i, 0);
+            one(f.a, f.b, f.o, f.m);
+        }
+    }
+    if constexpr (FPE) flush_flags(bits, flags);
+}
+
+// ---------------------------------------------------------------------------
+// unary
+// ---------------------------------------------------------------------------
+template <int OP, int CD, bool FPE>
+__global__ void __launch_bounds__(EW_THREADS)
+k_un_contig(const typename DT<CD>::T* __restrict__ a, typename UnOp<OP, CD>::R* __restrict__ o, int64_t n, uint32_t* flags) {
+    typedef typename DT<CD>::T T;
+    typedef typename UnOp<OP, CD>::R R;
+    constexpr int N = Vec16<T>::N;
+    constexpr int U = 2;
+    uint32_t bits = 0;
+    const int64_t nvec = n / N;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    for (; v + (U - 1) * stride < nvec; v += U * stride) {
+        Vec16<T> xa[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) xa[u] = ldv(a, v + u * stride);
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            R r[N];
+#pragma unroll
+            for (int k = 0; k < N; ++k) {
+                r[k] = UnOp<OP, CD>::apply(xa[u].v[k]);
+                if constexpr (FPE) bits |= UnOp<OP, CD>::fpe(xa[u].v[k]);
+            }
+            stv<R, N>(o, v + u * stride, r);
+        }
+    }
+    for (; v < nvec; v += stride) {
+        Vec16<T> xa = ldv(a, v);
+        R r[N];
+#pragma unroll
+        for (int k = 0; k < N; ++k) {
+            r[k] = UnOp<OP, CD>::apply(xa.v[k]);
+            if constexpr (FPE) bits |= UnOp<OP, CD>::fpe(xa.v[k]);
+        }
+        stv<R, N>(o, v, r);
+    }
+    for (int64_t i = nvec * N + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+        T x = a[i];
+        o[i] = UnOp<OP, CD>::apply(x);
+        if constexpr (FPE) bits |= UnOp<OP, CD>::fpe(x);
+    }
+    if constexpr (FPE) flush_flags(bits, flags);
+}
+
+template <int OP, int CD, bool FPE>
+__global__ void __launch_bounds__(EW_THREADS)
+k_un_nd(EwDesc d, uint32_t* flags) {
+    typedef typename DT<CD>::T T;
+    typedef UnOp<OP, CD> Op;
+    typedef typename Op::R R;
+    uint32_t bits = 0;
+    const int nd = d.nd;
+    const int64_t inner = d.shape[nd - 1];
+    const int64_t sa = d.a.st[nd - 1], so = d.so[nd - 1], sm = d.m.st[nd - 1];
+    const bool has_m = d.m.p != nullptr;
+    auto one = [&](int64_t oa, int64_t oo, int64_t om) {
+        T x = load_cast<CD>(d.a.p, oa, d.a.dt);
+        R r = Op::apply(x);
+        if constexpr (FPE) bits |= Op::fpe(x);
+        if (has_m && !((const uint8_t*)d.m.p)[om]) return;
+        store_cast<Op::OUT_DT>(d.o, oo, d.odt, r);
+    };
+    if (inner >= 64) {
+        constexpr int ILP = 4;
+        const int64_t tile = (int64_t)blockDim.x * ILP;
+        const int64_t tpr = (inner + tile - 1) / tile;
+        const int64_t ntiles = (d.n / inner) * tpr;
+        for (int64_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
+            int64_t row = t / tpr, cb = t - row * tpr;
+            Offs base = unravel(d, row, 1);
+            int64_t c0 = cb * tile + threadIdx.x;
+#pragma unroll
+            for (int u = 0; u < ILP; ++u) {
+                int64_t c = c0 + u * blockDim.x;
+                if (c < inner) one(base.a + c * sa, base.o + c * so, base.m + c * sm);
+            }
+        }
+    } else {
+        const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+        for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < d.n; i += stride) {
+            Offs f = unravel(d, i, 0);
+            one(f.a, f.o, f.m);
+        }
+    }
+    if constexpr (FPE) flush_flags(bits, flags);
+}
+
+// Grid size for a grid-stride element-wise launch: enough CTAs to fill all
+// 148 SMs at full occupancy, fewer for small problems.
+inline int ew_grid(int64_t work_items) {
+    int64_t want = (work_items + EW_THREADS - 1) / EW_THREADS;
+    int64_t cap = 148LL * 8;  // 8 resident 256-thread CTAs per SM
+    if (want < 1) want = 1;
+    return (int)(want < cap ? want : cap);
+}
+
+}  // namespace ionp

@@ -1,0 +1,74 @@
+// Launch helpers that instantiate the element-wise kernels for the legal
+// (op, loop dtype) pairs of the reference's dtype tables.
+#pragma once
+#include "ionp_ew.cuh"
+
+namespace ionp {
+
+// Loop dtypes each binary op can be dispatched on (binary_out_dtype,
+// ufunc.rs:1101, and the int_same / bool_same / float_same arms that exist).
+template <int OP, int CD> constexpr bool bin_valid() {
+    if (op_is_compare(OP)) return true;
+    if (op_is_logical(OP)) return CD == DT_BOOL;
+    if (OP == OP_ADD || OP == OP_MULTIPLY || OP == OP_MAXIMUM || OP == OP_MINIMUM) return true;
+    if (OP == OP_SUBTRACT) return CD != DT_BOOL;
+    if (OP == OP_DIVIDE) return dt_is_float(CD);
+    if (OP == OP_BITWISE_AND || OP == OP_BITWISE_OR || OP == OP_BITWISE_XOR) return !dt_is_float(CD);
+    if (OP == OP_LEFT_SHIFT || OP == OP_RIGHT_SHIFT) return dt_is_sint(CD) || dt_is_uint(CD);
+    if (OP == OP_FLOOR_DIVIDE || OP == OP_REMAINDER || OP == OP_FMOD) return CD != DT_BOOL;
+    return false;
+}
+
+template <int OP, int CD>
+cudaError_t launch_bin_t(const EwDesc& d, const ContigInfo& ci, uint32_t* flags, cudaStream_t s) {
+    typedef typename DT<CD>::T T;
+    typedef typename BinOp<OP, CD>::R R;
+    constexpr bool HAS_FPE = FpeKind<OP, CD>::value != 0;
+    const bool fpe = HAS_FPE && flags != nullptr;
+    if (d.n == 0) return cudaSuccess;
+    if (ci.ok) {
+        int64_t nv = d.n / Vec16<T>::N;
+        int g = ew_grid(nv > 0 ? (nv + 1) / 2 : d.n);
+        const T* a = (const T*)d.a.p;
+        const T* b = (const T*)d.b.p;
+        R* o = (R*)d.o;
+        if constexpr (HAS_FPE) {
+            if (fpe) { k_bin_contig<OP, CD, true><<<g, EW_THREADS, 0, s>>>(a, b, o, d.n, ci.a_scalar, ci.b_scalar, flags); count_launch(); return cudaGetLastError(); }
+        }
+        k_bin_contig<OP, CD, false><<<g, EW_THREADS, 0, s>>>(a, b, o, d.n, ci.a_scalar, ci.b_scalar, flags);
+        count_launch();
+        return cudaGetLastError();
+    }
+    const bool same = d.a.dt == CD && d.b.dt == CD && d.odt == BinOp<OP, CD>::OUT_DT && d.m.p == nullptr;
+    int64_t inner = d.shape[d.nd - 1];
+    int g = ew_grid(inner >= 64 ? (d.n + 3) / 4 : d.n);
+    if constexpr (HAS_FPE) {
+        if (fpe) {
+            if (same) k_bin_nd<OP, CD, true, true><<<g, EW_THREADS, 0, s>>>(d, flags);
+            else k_bin_nd<OP, CD, true, false><<<g, EW_THREADS, 0, s>>>(d, flags);
+            count_launch();
+            return cudaGetLastError();
+        }
+    }
+    if (same) k_bin_nd<OP, CD, false, true><<<g, EW_THREADS, 0, s>>>(d, flags);
+    else k_bin_nd<OP, CD, false, false><<<g, EW_THREADS, 0, s>>>(d, flags);
+    count_launch();
+    return cudaGetLastError();
+}
+
+template <int OP>
+cudaError_t launch_bin_op(int cd, const EwDesc& d, const ContigInfo& ci, uint32_t* flags, cudaStream_t s) {
+#define IONP_CASE(D)                                                             \
+    case D:                                                                      \
+        if constexpr (bin_valid<OP, D>()) return launch_bin_t<OP, D>(d, ci, flags, s); \
+        break;
+    switch (cd) {
+        IONP_CASE(DT_BOOL) IONP_CASE(DT_I8) IONP_CASE(DT_I16) IONP_CASE(DT_I32) IONP_CASE(DT_I64)
+        IONP_CASE(DT_U8) IONP_CASE(DT_U16) IONP_CASE(DT_U32) IONP_CASE(DT_U64)
+        IONP_CASE(DT_F16) IONP_CASE(DT_F32) IONP_CASE(DT_F64)
+    }
+#undef IONP_CASE
+    return cudaErrorInvalidValue;
+}
+
+}  // namespace ionp

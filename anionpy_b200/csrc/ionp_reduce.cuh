@@ -1,0 +1,809 @@
+// Reduction and argmin/argmax kernels (ufunc.reduce / argext hot path).
+//
+// Fold orders follow the reference exactly (ionp-core/src/ufunc.rs):
+//  * float add on the "wide" run (the reduced axes that are the smallest-
+//    stride axes of the whole array) is numpy's pairwise sum: recursive
+//    halving at n/2 rounded down to a multiple of 8 until a block of <= 128,
+//    each block summed by 8 strided accumulators combined as
+//    ((r0+r1)+(r2+r3))+((r4+r5)+(r6+r7)), tail added in order
+//    (pairwise_sum, ufunc.rs:6416-6448);
+//  * "narrow" reduced axes fold sequentially in memory order, seeded with the
+//    identity or initial (ufunc.rs:6658-6806);
+//  * float16 add/multiply/subtract/divide widen to f32 on the wide run and
+//    round to f16 per narrow step (ufunc.rs:6868-7089);
+//  * everything else is a sequential fold in ascending-axis C order
+//    (sequential_group, ufunc.rs:6546), in memory order for float multiply
+//    (sequential_group_ordered, ufunc.rs:6583).
+//
+// Kernels:
+//  k_red_row   : one output per thread group; the group's elements form one
+//                strided run. The pairwise tree is rebuilt on the device:
+//                every group of 8 threads ("octet") locates a leaf block by
+//                descending the split tree from the root, sums it with the 8
+//                accumulators, and parks the result in a shared-memory slot
+//                array laid out as a perfect binary tree (a leaf at depth d
+//                with path p sits at slot p << (D - d)); the tree is then
+//                combined level by level, left operand first. Associative
+//                ops (int add, max, bitwise, ...) reuse the same kernel: any
+//                order-preserving bracketing gives identical bits for them.
+//                Runs longer than one CTA's segment are cut at a fixed tree
+//                depth K (every node above K is an interior node), each
+//                subtree reduced by its own CTA into scratch, and the top K
+//                levels combined by a second launch.
+//  k_red_col   : one output per thread, sequential over the reduced offsets
+//                (narrow axes, or any op without a pairwise loop); adjacent
+//                threads own adjacent outputs so loads coalesce along the
+//                kept axis.
+//  k_red_gen   : one output per thread, the general wide x narrow nest with
+//                several wide runs, for the layouts that need it.
+//  k_red_masked: where= reductions (ufunc.rs:7213-7548), one output per thread.
+//  k_argext_*  : argmin/argmax with (value, index) pairs, first occurrence on
+//                ties and first NaN winning (ufunc.rs:8037-8206).
+#pragma once
+#include "ionp_scalar.cuh"
+#include "ionp_internal.h"
+
+namespace ionp {
+
+constexpr int RD_MAXD = 8;
+constexpr int RED_THREADS = 256;
+constexpr int PW_BLOCK = 128;
+
+// Reduction launch descriptor (by value).
+struct RedDesc {
+    const void* a;   // input, first element
+    int32_t adt;     // input dtype (cast on load to the compute dtype)
+    int32_t cd;      // compute dtype
+    int32_t op;
+    int64_t nout;    // outputs (product of kept dims)
+    int32_t nk;      // kept dims, C order = output order
+    int64_t kshape[RD_MAXD], kst[RD_MAXD], kost[RD_MAXD];
+    // ROW: the group is one run of `w` elements at stride `ws`.
+    int64_t w, ws;
+    // COL / GEN: narrow dims in fold order (outermost first)
+    int32_t nr;
+    int64_t rshape[RD_MAXD], rst[RD_MAXD];
+    // GEN: wide runs innermost first (runs[0] pairwise, runs[1..] outer)
+    int32_t nw;
+    int64_t wshape[RD_MAXD], wst[RD_MAXD];
+    int32_t has_seed;
+    uint64_t seed;   // bits of the seed in the compute dtype
+    void* o;         // output first element
+    int32_t odt;
+    // split ROW (K > 0): partials scratch, nout x 2^K accumulators
+    int32_t K;
+    int32_t D;       // slot-tree depth of one segment
+    void* scratch;
+    // masked
+    const uint8_t* m;
+    int64_t mkst[RD_MAXD], mrst[RD_MAXD], mwst_raw[RD_MAXD];
+    int32_t nwr;     // masked: raw (uncoalesced) wide dims, innermost last
+    int64_t wrshape[RD_MAXD], wrst[RD_MAXD];
+    int32_t pairwise;  // masked: float add family
+};
+
+// Loads of the only cast the reduction kernels do on the fly: add/multiply
+// widening bool and narrower integers to int64/uint64
+// (reduce_compute_dtype, ufunc.rs:2041-2078). Other casts are materialised.
+template <int CD> __device__ __forceinline__ typename DT<CD>::T load_int_widen(const void* p, int64_t e, int sdt) {
+    typedef typename DT<CD>::T T;
+    switch (sdt) {
+        case DT_BOOL: return (T)(((const uint8_t*)p)[e] != 0);
+        case DT_I8: return (T)((const int8_t*)p)[e];
+        case DT_I16: return (T)((const int16_t*)p)[e];
+        case DT_I32: return (T)((const int32_t*)p)[e];
+        case DT_U8: return (T)((const uint8_t*)p)[e];
+        case DT_U16: return (T)((const uint16_t*)p)[e];
+        case DT_U32: return (T)((const uint32_t*)p)[e];
+        default: return ((const T*)p)[e];
+    }
+}
+
+// Accumulation policy of the pairwise/tree kernels.
+template <int OP, int CD, bool CASTLD = false> struct RPol {
+    static constexpr bool F16W = (CD == DT_F16 && OP == OP_ADD);
+    static constexpr int AD = F16W ? DT_F32 : CD;
+    typedef typename DT<CD>::T T;
+    typedef typename DT<AD>::T A;
+    static __device__ __forceinline__ A fold(A x, A y) { return BinOp<OP, AD>::apply(x, y); }
+    static __device__ __forceinline__ A load(const void* p, int64_t e, int sdt) {
+        if constexpr (CASTLD) return load_int_widen<CD>(p, e, sdt);
+        else if constexpr (F16W) return h2f(((const h16*)p)[e]);
+        else return ((const T*)p)[e];
+    }
+    // the result of one output from its tree total
+    static __device__ __forceinline__ T finish(A total, int has_seed, uint64_t seed_bits) {
+        if constexpr (F16W) {
+            h16 s = (h16)seed_bits;  // add always has a seed (0 or initial)
+            return FOps<DT_F16>::add(s, f2h(total));
+        } else {
+            if (has_seed) {
+                T s;
+                memcpy(&s, &seed_bits, sizeof(T));
+                return BinOp<OP, CD>::apply(s, total);
+            }
+            return total;
+        }
+    }
+};
+
+__host__ __device__ __forceinline__ int64_t pw_split(int64_t len) {
+    int64_t n2 = len / 2;
+    return n2 - n2 % 8;
+}
+
+// Offsets of output index `o` over the kept dims: input and output.
+__device__ __forceinline__ void kept_offsets(const RedDesc& d, int64_t o, int64_t* in_off, int64_t* out_off) {
+    int64_t a = 0, b = 0;
+    for (int k = d.nk - 1; k >= 0; --k) {
+        int64_t s = d.kshape[k];
+        int64_t q = o / s;
+        int64_t id = o - q * s;
+        o = q;
+        a += id * d.kst[k];
+        b += id * d.kost[k];
+    }
+    *in_off = a;
+    *out_off = b;
+}
+
+// Descend K levels of the split tree of a run of n along `path`.
+__device__ __forceinline__ void seg_of(int64_t n, int K, int64_t path, int64_t* off, int64_t* len) {
+    int64_t o = 0, l = n;
+    for (int k = K - 1; k >= 0; --k) {
+        int64_t n2 = pw_split(l);
+        if ((path >> k) & 1) { o += n2; l -= n2; } else { l = n2; }
+    }
+    *off = o;
+    *len = l;
+}
+
+// Sum one leaf block [off, off+len) (len <= 128, len >= 8) with one octet.
+// Returns the octet's combined value in lane 0 of the octet (lane j of the
+// octet holds accumulator j before the combine).
+template <class P>
+__device__ __forceinline__ typename P::A leaf_octet(const void* p, int sdt, int64_t base, int64_t ws, int64_t off, int64_t len, int j) {
+    typedef typename P::A A;
+    const int64_t lim = len - len % 8;
+    A r = P::load(p, base + (off + j) * ws, sdt);
+    A x[15];
+#pragma unroll
+    for (int i = 0; i < 15; ++i) {
+        int64_t e = off + 8 * (i + 1) + j;
+        if (8 * (i + 1) < lim) x[i] = P::load(p, base + e * ws, sdt);
+    }
+#pragma unroll
+    for (int i = 0; i < 15; ++i)
+        if (8 * (i + 1) < lim) r = P::fold(r, x[i]);
+    // ((r0+r1)+(r2+r3))+((r4+r5)+(r6+r7)): lower lane is the left operand
+    const unsigned mask = 0xFFu << ((threadIdx.x & 31) & ~7u);
+#pragma unroll
+    for (int s = 1; s < 8; s <<= 1) {
+        A other = __shfl_down_sync(mask, r, s, 8);
+        if ((j & (2 * s - 1)) == 0) r = P::fold(r, other);
+    }
+    if (j == 0) {
+        for (int64_t i = lim; i < len; ++i) r = P::fold(r, P::load(p, base + (off + i) * ws, sdt));
+    }
+    return r;
+}
+
+// Barrier over one TPR-thread group (a CTA-wide barrier when TPR > 32).
+template <int TPR> __device__ __forceinline__ void group_sync() {
+    if constexpr (TPR > 32) __syncthreads();
+    else if constexpr (TPR == 32) __syncwarp();
+    else __syncwarp(((1u << TPR) - 1u) << ((threadIdx.x & 31) & ~(unsigned)(TPR - 1)));
+}
+
+// One output group of TPR threads reduces the run [seg_off, seg_off+n) of
+// output row `base` with the pairwise tree; result valid in the group's
+// thread 0. `slots`/`valid` are this group's 2^D shared-memory slots.
+template <class P, int TPR>
+__device__ typename P::A group_tree(const RedDesc& d, int64_t base, int64_t seg_off, int64_t n, int D,
+                                    typename P::A* slots, uint8_t* valid, int t) {
+    typedef typename P::A A;
+    const int ws = 0;
+    (void)ws;
+    if (n < 8) {
+        A r{};
+        if (t == 0 && n > 0) {
+            r = P::load(d.a, base + seg_off * d.ws, d.adt);
+            for (int64_t i = 1; i < n; ++i) r = P::fold(r, P::load(d.a, base + (seg_off + i) * d.ws, d.adt));
+        }
+        return r;
+    }
+    const int oct = t >> 3, j = t & 7;
+    constexpr int NOCT = TPR / 8;
+    if (n <= PW_BLOCK) {
+        A r{};
+        if (oct == 0) r = leaf_octet<P>(d.a, d.adt, base, d.ws, seg_off, n, j);
+        return r;
+    }
+    const int nslots = 1 << D;
+    for (int s = t; s < nslots; s += TPR) valid[s] = 0;
+    group_sync<TPR>();
+    const int64_t ncand = (n + 63) / 64;
+    for (int64_t c0 = 0; c0 < ncand; c0 += NOCT) {
+        int64_t c = c0 + oct;
+        int64_t off = 0, len = n, path = 0;
+        int depth = 0;
+        bool own = false;
+        if (c < ncand) {
+            int64_t m = c * 64;
+            while (len > PW_BLOCK) {
+                int64_t n2 = pw_split(len);
+                path <<= 1;
+                depth++;
+                if (m < off + n2) len = n2; else { off += n2; len -= n2; path |= 1; }
+            }
+            own = off > m - 64;
+        }
+        // octets are warp-aligned; the whole octet agrees on `own`
+        if (own) {
+            A r = leaf_octet<P>(d.a, d.adt, base, d.ws, seg_off + off, len, j);
+            if (j == 0) {
+                int s = (int)(path << (D - depth));
+                slots[s] = r;
+                valid[s] = 1;
+            }
+        }
+    }
+    group_sync<TPR>();
+    for (int lvl = D - 1; lvl >= 0; --lvl) {
+        const int half = 1 << (D - 1 - lvl), step = half * 2;
+        for (int s = t * step; s < nslots; s += TPR * step) {
+            if (valid[s + half]) slots[s] = P::fold(slots[s], slots[s + half]);
+        }
+        group_sync<TPR>();
+    }
+    return slots[0];
+}
+
+// ROW kernel. Tasks = nout x 2^K; each TPR-thread group takes one task.
+template <int OP, int CD, int TPR, bool CASTLD>
+__global__ void __launch_bounds__(RED_THREADS) k_red_row(RedDesc d) {
+    typedef RPol<OP, CD, CASTLD> P;
+    typedef typename P::A A;
+    typedef typename P::T T;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    constexpr int GROUPS = RED_THREADS / TPR;
+    const int g = threadIdx.x / TPR, t = threadIdx.x % TPR;
+    const int nslots = TPR >= 16 ? (1 << d.D) : 1;
+    A* slots = reinterpret_cast<A*>(smem_raw) + (size_t)g * nslots;
+    uint8_t* valid = reinterpret_cast<uint8_t*>(reinterpret_cast<A*>(smem_raw) + (size_t)GROUPS * nslots) + (size_t)g * nslots;
+    const int64_t nseg = (int64_t)1 << d.K;
+    const int64_t ntasks = d.nout * nseg;
+    // all groups of a CTA iterate the same number of times (TPR > 32 syncs)
+    for (int64_t t0 = (int64_t)blockIdx.x * GROUPS; t0 < ntasks; t0 += (int64_t)gridDim.x * GROUPS) {
+        int64_t task = t0 + g;
+        bool live = task < ntasks;
+        int64_t o = live ? task / nseg : 0, sg = live ? task % nseg : 0;
+        int64_t in_off, out_off;
+        kept_offsets(d, o, &in_off, &out_off);
+        int64_t soff, slen;
+        seg_of(d.w, d.K, sg, &soff, &slen);
+        if (!live) slen = 0;
+        A r{};
+        if constexpr (TPR > 32) {
+            r = group_tree<P, TPR>(d, in_off, soff, slen, d.D, slots, valid, t);
+        } else {
+            if (slen > 0) r = group_tree<P, TPR>(d, in_off, soff, slen, d.D, slots, valid, t);
+        }
+        if (live && t == 0) {
+            if (d.K == 0) store_cast<CD>(d.o, out_off, d.odt, P::finish(r, d.has_seed, d.seed));
+            else reinterpret_cast<A*>(d.scratch)[task] = r;
+        }
+        if constexpr (TPR > 32) __syncthreads();
+    }
+}
+
+// Top of a split tree: per output, combine its 2^K partials as a perfect
+// binary tree (adjacent pairs, left operand first), then seed and store.
+template <int OP, int CD>
+__global__ void __launch_bounds__(RED_THREADS) k_red_row_top(RedDesc d) {
+    typedef RPol<OP, CD> P;
+    typedef typename P::A A;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    A* v = reinterpret_cast<A*>(smem_raw);
+    const int nseg = 1 << d.K;
+    for (int64_t o = blockIdx.x; o < d.nout; o += gridDim.x) {
+        const A* part = reinterpret_cast<const A*>(d.scratch) + o * nseg;
+        for (int s = threadIdx.x; s < nseg; s += blockDim.x) v[s] = part[s];
+        __syncthreads();
+        for (int half = 1; half < nseg; half <<= 1) {
+            for (int s = threadIdx.x * 2 * half; s < nseg; s += blockDim.x * 2 * half) v[s] = P::fold(v[s], v[s + half]);
+            __syncthreads();
+        }
+        if (threadIdx.x == 0) {
+            int64_t in_off, out_off;
+            kept_offsets(d, o, &in_off, &out_off);
+            store_cast<CD>(d.o, out_off, d.odt, P::finish(v[0], d.has_seed, d.seed));
+        }
+        __syncthreads();
+    }
+}
+
+// COL kernel: sequential fold per output over the narrow dims (fold order).
+template <int OP, int CD, bool CASTLD>
+__global__ void __launch_bounds__(RED_THREADS) k_red_col(RedDesc d) {
+    typedef typename DT<CD>::T T;
+    typedef RPol<OP, CD, CASTLD> P;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    int64_t total = 1;
+    for (int k = 0; k < d.nr; ++k) total *= d.rshape[k];
+    const int64_t rs_in = d.nr > 0 ? d.rst[d.nr - 1] : 0;
+    const int64_t rn_in = d.nr > 0 ? d.rshape[d.nr - 1] : 1;
+    for (int64_t o = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; o < d.nout; o += stride) {
+        int64_t base, out_off;
+        kept_offsets(d, o, &base, &out_off);
+        bool have = d.has_seed;
+        T acc;
+        memcpy(&acc, &d.seed, sizeof(T));
+        // walk the narrow dims: outer dims by odometer, innermost unrolled
+        int64_t idx[RD_MAXD] = {0};
+        int64_t outer_off = 0;
+        for (int64_t done = 0; done < total; done += rn_in) {
+            const int64_t b0 = base + outer_off;
+            int64_t j = 0;
+            constexpr int U = 8;
+            for (; j + U <= rn_in; j += U) {
+                T x[U];
+#pragma unroll
+                for (int u = 0; u < U; ++u) {
+                    if constexpr (CASTLD) x[u] = load_int_widen<CD>(d.a, b0 + (j + u) * rs_in, d.adt);
+                    else x[u] = ((const T*)d.a)[b0 + (j + u) * rs_in];
+                }
+#pragma unroll
+                for (int u = 0; u < U; ++u) {
+                    if (!have) { acc = x[u]; have = true; }
+                    else acc = BinOp<OP, CD>::apply(acc, x[u]);
+                }
+            }
+            for (; j < rn_in; ++j) {
+                T x;
+                if constexpr (CASTLD) x = load_int_widen<CD>(d.a, b0 + j * rs_in, d.adt);
+                else x = ((const T*)d.a)[b0 + j * rs_in];
+                if (!have) { acc = x; have = true; }
+                else acc = BinOp<OP, CD>::apply(acc, x);
+            }
+            for (int k = d.nr - 2; k >= 0; --k) {
+                idx[k]++;
+                outer_off += d.rst[k];
+                if (idx[k] < d.rshape[k]) break;
+                outer_off -= d.rst[k] * d.rshape[k];
+                idx[k] = 0;
+            }
+        }
+        store_cast<CD>(d.o, out_off, d.odt, acc);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Per-thread pairwise sum (iterative, explicit stack) for the general paths.
+// get(i) returns element i of the run as the accumulator type.
+// ---------------------------------------------------------------------------
+template <class A, class Get, class Fold>
+__device__ A pw_thread(Get get, int64_t n, Fold fold) {
+    auto leaf = [&](int64_t b, int64_t len) -> A {
+        if (len < 8) {
+            A r = get(b);
+            for (int64_t i = 1; i < len; ++i) r = fold(r, get(b + i));
+            return r;
+        }
+        A r[8];
+        for (int k = 0; k < 8; ++k) r[k] = get(b + k);
+        int64_t i = 8;
+        for (; i < len - len % 8; i += 8)
+            for (int k = 0; k < 8; ++k) r[k] = fold(r[k], get(b + i + k));
+        A res = fold(fold(fold(r[0], r[1]), fold(r[2], r[3])), fold(fold(r[4], r[5]), fold(r[6], r[7])));
+        for (; i < len; ++i) res = fold(res, get(b + i));
+        return res;
+    };
+    if (n <= PW_BLOCK) return leaf(0, n);
+    // post-order walk; frame: node (b, len), state 0 = descend left,
+    // 1 = descend right (left value saved), 2 = combine
+    int64_t fb_[48], fl_[48];
+    A fv[48];
+    uint8_t fs[48];
+    int sp = 0;
+    fb_[0] = 0; fl_[0] = n; fs[0] = 0;
+    A ret{};
+    while (sp >= 0) {
+        int64_t b = fb_[sp], len = fl_[sp];
+        if (len <= PW_BLOCK) {
+            ret = leaf(b, len);
+            --sp;
+            continue;
+        }
+        int64_t n2 = pw_split(len);
+        if (fs[sp] == 0) {
+            fs[sp] = 1;
+            ++sp; fb_[sp] = b; fl_[sp] = n2; fs[sp] = 0;
+        } else if (fs[sp] == 1) {
+            fv[sp] = ret;
+            fs[sp] = 2;
+            ++sp; fb_[sp] = b + n2; fl_[sp] = len - n2; fs[sp] = 0;
+        } else {
+            ret = fold(fv[sp], ret);
+            --sp;
+        }
+    }
+    return ret;
+}
+
+// GEN kernel: one output per thread, the full narrow x wide nest.
+// float add (f32/f64): reduce_axis_pairwise_narrow_wide (ufunc.rs:6658).
+// float16 add/mul/sub/div: reduce_axis_f16_narrow_wide (ufunc.rs:6868).
+template <int OP, int CD>
+__global__ void __launch_bounds__(128) k_red_gen(RedDesc d) {
+    typedef typename DT<CD>::T T;
+    constexpr bool F16 = CD == DT_F16;
+    typedef typename std::conditional<F16, float, T>::type A;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    int64_t ntotal = 1;
+    for (int k = 0; k < d.nr; ++k) ntotal *= d.rshape[k];
+    for (int64_t o = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; o < d.nout; o += stride) {
+        int64_t base, out_off;
+        kept_offsets(d, o, &base, &out_off);
+        auto ld = [&](int64_t e) -> A {
+            if constexpr (F16) return h2f(((const h16*)d.a)[e]);
+            else return ((const T*)d.a)[e];
+        };
+        auto afold = [&](A x, A y) -> A {
+            if constexpr (F16) return BinOp<OP, DT_F32>::apply(x, y);
+            else return BinOp<OP, CD>::apply(x, y);
+        };
+        // pairwise_group (ufunc.rs:6504): inner run pairwise, outer runs
+        // folded sequentially in NdIter order over runs[1..] (runs[1] slowest)
+        auto wide_pairwise = [&](int64_t wb) -> A {
+            if (d.nw == 0) return ld(wb);
+            const int64_t isz = d.wshape[0], ist = d.wst[0];
+            auto inner = [&](int64_t b) { return pw_thread<A>([&](int64_t i) { return ld(b + ist * i); }, isz, afold); };
+            if (d.nw == 1) return inner(wb);
+            int64_t nouter = 1;
+            for (int k = 1; k < d.nw; ++k) nouter *= d.wshape[k];
+            A acc{};
+            for (int64_t q = 0; q < nouter; ++q) {
+                int64_t rem = q, off = 0;
+                for (int k = d.nw - 1; k >= 1; --k) {
+                    int64_t id = rem % d.wshape[k];
+                    rem /= d.wshape[k];
+                    off += id * d.wst[k];
+                }
+                A v = inner(wb + off);
+                acc = q == 0 ? v : afold(acc, v);
+            }
+            return acc;
+        };
+        // sequential over the wide elements in C order (outermost run first)
+        auto wide_seq = [&](int64_t wb, bool seeded, A s) -> A {
+            int64_t nel = 1;
+            for (int k = 0; k < d.nw; ++k) nel *= d.wshape[k];
+            A acc = s;
+            bool have = seeded;
+            for (int64_t q = 0; q < nel; ++q) {
+                int64_t rem = q, off = 0;
+                for (int k = 0; k < d.nw; ++k) {
+                    int64_t id = rem % d.wshape[k];
+                    rem /= d.wshape[k];
+                    off += id * d.wst[k];
+                }
+                A v = ld(wb + off);
+                if (!have) { acc = v; have = true; } else acc = afold(acc, v);
+            }
+            return acc;
+        };
+        auto compute_wide = [&](int64_t wb) -> A {
+            if (d.nw == 0) return ld(wb);
+            if constexpr (F16) { if (OP != OP_ADD) return wide_seq(wb, false, A{}); }
+            return wide_pairwise(wb);
+        };
+        T res;
+        T seedv;
+        memcpy(&seedv, &d.seed, sizeof(T));
+        if (d.nr == 0) {
+            if constexpr (F16) {
+                if (d.has_seed && OP != OP_ADD) res = f2h(wide_seq(base, true, h2f(seedv)));
+                else if (d.has_seed) res = BinOp<OP, DT_F16>::apply(seedv, f2h(compute_wide(base)));
+                else res = f2h(compute_wide(base));
+            } else {
+                res = BinOp<OP, CD>::apply(seedv, compute_wide(base));  // float add: seed always present
+            }
+        } else {
+            bool have = d.has_seed;
+            T acc = seedv;
+            for (int64_t q = 0; q < ntotal; ++q) {
+                int64_t rem = q, off = 0;
+                for (int k = d.nr - 1; k >= 0; --k) {
+                    int64_t id = rem % d.rshape[k];
+                    rem /= d.rshape[k];
+                    off += id * d.rst[k];
+                }
+                T part;
+                if constexpr (F16) part = f2h(compute_wide(base + off));
+                else part = compute_wide(base + off);
+                if (!have) { acc = part; have = true; } else acc = BinOp<OP, CD>::apply(acc, part);
+            }
+            res = acc;
+        }
+        store_cast<CD>(d.o, out_off, d.odt, res);
+    }
+}
+
+// Masked reductions (reduce_axis_masked, ufunc.rs:7213-7412, and
+// reduce_axis_masked_f16_widen, 7414-7548). The seed always exists here.
+template <int OP, int CD>
+__global__ void __launch_bounds__(128) k_red_masked(RedDesc d) {
+    typedef typename DT<CD>::T T;
+    constexpr bool F16W = CD == DT_F16 && (OP == OP_ADD || OP == OP_MULTIPLY || OP == OP_SUBTRACT || OP == OP_DIVIDE);
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    T seedv;
+    memcpy(&seedv, &d.seed, sizeof(T));
+    for (int64_t o = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; o < d.nout; o += stride) {
+        // kept offsets for data and mask
+        int64_t base = 0, mbase = 0, out_off = 0;
+        {
+            int64_t r = o;
+            for (int k = d.nk - 1; k >= 0; --k) {
+                int64_t id = r % d.kshape[k];
+                r /= d.kshape[k];
+                base += id * d.kst[k];
+                mbase += id * d.mkst[k];
+                out_off += id * d.kost[k];
+            }
+        }
+        int64_t nn = 1;
+        for (int k = 0; k < d.nr; ++k) nn *= d.rshape[k];
+        int64_t nwe = 1;
+        for (int k = 0; k < d.nwr; ++k) nwe *= d.wrshape[k];
+        auto woff = [&](int64_t q, int64_t* dof, int64_t* mof) {
+            int64_t rem = q, a = 0, m = 0;
+            for (int k = d.nwr - 1; k >= 0; --k) {
+                int64_t id = rem % d.wrshape[k];
+                rem /= d.wrshape[k];
+                a += id * d.wrst[k];
+                m += id * d.mwst_raw[k];
+            }
+            *dof = a; *mof = m;
+        };
+        auto noff = [&](int64_t q, int64_t* dof, int64_t* mof) {
+            int64_t rem = q, a = 0, m = 0;
+            for (int k = d.nr - 1; k >= 0; --k) {
+                int64_t id = rem % d.rshape[k];
+                rem /= d.rshape[k];
+                a += id * d.rst[k];
+                m += id * d.mrst[k];
+            }
+            *dof = a; *mof = m;
+        };
+        constexpr bool PW = F16W || (OP == OP_ADD && (CD == DT_F32 || CD == DT_F64));
+        if constexpr (PW) {
+            typedef typename std::conditional<F16W, float, T>::type A;
+            auto ld = [&](int64_t e) -> A {
+                if constexpr (F16W) return h2f(((const h16*)d.a)[e]);
+                else return ((const T*)d.a)[e];
+            };
+            auto afold = [&](A x, A y) -> A {
+                if constexpr (F16W) return BinOp<OP, DT_F32>::apply(x, y);
+                else return BinOp<OP, CD>::apply(x, y);
+            };
+            // compute_wide_masked over the raw wide dims (C order)
+            auto cwm = [&](int64_t wb, int64_t mwb, A acc_in) -> A {
+                if (d.nwr == 0) {
+                    if (!d.m[mwb]) return acc_in;
+                    if constexpr (F16W) return h2f(f2h(afold(acc_in, ld(wb))));
+                    else return afold(acc_in, ld(wb));
+                }
+                A acc = acc_in;
+                int64_t q = 0;
+                while (q < nwe) {
+                    int64_t dof, mof;
+                    woff(q, &dof, &mof);
+                    if (!d.m[mwb + mof]) { ++q; continue; }
+                    int64_t q1 = q + 1;
+                    for (; q1 < nwe; ++q1) { woff(q1, &dof, &mof); if (!d.m[mwb + mof]) break; }
+                    int64_t len = q1 - q;
+                    auto get = [&](int64_t i) { int64_t a_, m_; woff(q + i, &a_, &m_); return ld(wb + a_); };
+                    A comb;
+                    if constexpr (F16W) {
+                        if (OP == OP_ADD) comb = afold(acc, pw_thread<A>(get, len, afold));
+                        else if (OP == OP_MULTIPLY) {
+                            A r = get(0);
+                            for (int64_t i = 1; i < len; ++i) r = afold(r, get(i));
+                            comb = afold(acc, r);
+                        } else {
+                            A r = acc;
+                            for (int64_t i = 0; i < len; ++i) r = afold(r, get(i));
+                            comb = r;
+                        }
+                        acc = h2f(f2h(comb));
+                    } else {
+                        acc = afold(acc, pw_thread<A>(get, len, afold));
+                    }
+                    q = q1;
+                }
+                return acc;
+            };
+            A acc;
+            if constexpr (F16W) acc = h2f(seedv); else acc = seedv;
+            if (d.nr == 0) acc = cwm(base, mbase, acc);
+            else {
+                for (int64_t q = 0; q < nn; ++q) {
+                    int64_t dof, mof;
+                    noff(q, &dof, &mof);
+                    acc = cwm(base + dof, mbase + mof, acc);
+                }
+            }
+            T res;
+            if constexpr (F16W) res = f2h(acc); else res = acc;
+            store_cast<CD>(d.o, out_off, d.odt, res);
+        } else {
+            // reduced axes in memory order; fold the masked-in elements
+            T acc = seedv;
+            for (int64_t q = 0; q < nn; ++q) {
+                int64_t dof, mof;
+                noff(q, &dof, &mof);
+                if (d.m[mbase + mof]) acc = BinOp<OP, CD>::apply(acc, ((const T*)d.a)[base + dof]);
+            }
+            store_cast<CD>(d.o, out_off, d.odt, acc);
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// argmin / argmax
+// ---------------------------------------------------------------------------
+template <int CD, bool MAX> struct ArgPol {
+    typedef typename DT<CD>::T T;
+    static __device__ __forceinline__ bool is_nan(T v) {
+        if constexpr (CD == DT_F16) return isnan_h(v);
+        else if constexpr (CD == DT_F32) return isnan_f(v);
+        else if constexpr (CD == DT_F64) return isnan_d(v);
+        else return false;
+    }
+    // (v, i) replaces (b, bi): strictly better, or not worse and earlier.
+    // Equals the first-best of a sequential scan in index order.
+    static __device__ __forceinline__ bool takes(T v, int64_t i, T b, int64_t bi) {
+        if (i < 0) return false;
+        if (bi < 0) return true;
+        if (better(v, b)) return true;
+        if (better(b, v)) return false;
+        return i < bi;
+    }
+    // better(v, best) of reduce_axis_argext (ufunc.rs:8139-8160)
+    static __device__ __forceinline__ bool better(T v, T b) {
+        bool c;
+        if constexpr (CD == DT_F16) c = MAX ? (h2f(v) > h2f(b)) : (h2f(v) < h2f(b));
+        else c = MAX ? (v > b) : (v < b);
+        if constexpr (dt_is_float(CD)) return c || (is_nan(v) && !is_nan(b));
+        else return c;
+    }
+};
+
+// One output per TPR-thread group; group elements: flat index i in [0, w),
+// offset = unravel(i) over (rshape, rst) (C order) -- the argext axis, or the
+// whole array for axis=None. Pairs combine left-first: the later pair only
+// wins when strictly better, which is associative and equals the sequential
+// scan.
+template <int CD, bool MAX, int TPR>
+__global__ void __launch_bounds__(RED_THREADS) k_argext(RedDesc d) {
+    typedef ArgPol<CD, MAX> P;
+    typedef typename DT<CD>::T T;
+    constexpr int GROUPS = RED_THREADS / TPR;
+    const int g = threadIdx.x / TPR, t = threadIdx.x % TPR;
+    const int64_t nseg = (int64_t)1 << d.K;
+    const int64_t ntasks = d.nout * nseg;
+    const int64_t seglen = (d.w + nseg - 1) / nseg;
+    for (int64_t t0 = (int64_t)blockIdx.x * GROUPS; t0 < ntasks; t0 += (int64_t)gridDim.x * GROUPS) {
+        int64_t task = t0 + g;
+        bool live = task < ntasks;
+        int64_t o = live ? task / nseg : 0, sg = live ? task % nseg : 0;
+        int64_t base, out_off;
+        kept_offsets(d, o, &base, &out_off);
+        int64_t lo = sg * seglen, hi = lo + seglen;
+        if (hi > d.w) hi = d.w;
+        if (!live) hi = lo;
+        T best{};
+        int64_t bi = -1;
+        for (int64_t i = lo + t; i < hi; i += TPR) {
+            int64_t off = 0, rem = i;
+            for (int k = d.nr - 1; k >= 0; --k) {
+                int64_t id = rem % d.rshape[k];
+                rem /= d.rshape[k];
+                off += id * d.rst[k];
+            }
+            T v = ((const T*)d.a)[base + off];
+            if (bi < 0 || P::better(v, best)) { best = v; bi = i; }
+        }
+        // combine across the group, lower lanes (earlier indices) first
+        if constexpr (TPR > 1) {
+            const unsigned mask = TPR >= 32 ? 0xFFFFFFFFu : (((1u << TPR) - 1u) << ((threadIdx.x & 31) & ~(unsigned)(TPR - 1)));
+            for (int s = 1; s < TPR && s < 32; s <<= 1) {
+                T ov = __shfl_down_sync(mask, best, s, TPR < 32 ? TPR : 32);
+                int64_t oi = __shfl_down_sync(mask, bi, s, TPR < 32 ? TPR : 32);
+                if ((t & (2 * s - 1)) == 0 && P::takes(ov, oi, best, bi)) { best = ov; bi = oi; }
+            }
+            if constexpr (TPR > 32) {
+                __shared__ T sv[RED_THREADS / 32];
+                __shared__ int64_t si[RED_THREADS / 32];
+                if ((t & 31) == 0) { sv[threadIdx.x / 32] = best; si[threadIdx.x / 32] = bi; }
+                __syncthreads();
+                if (t == 0) {
+                    for (int w = 1; w < TPR / 32; ++w) {
+                        int k = threadIdx.x / 32 + w;
+                        if (P::takes(sv[k], si[k], best, bi)) { best = sv[k]; bi = si[k]; }
+                    }
+                }
+                __syncthreads();
+            }
+        }
+        if (live && t == 0) {
+            if (d.K == 0) ((int64_t*)d.o)[out_off] = bi < 0 ? 0 : bi;
+            else {
+                int64_t* ixs = reinterpret_cast<int64_t*>(d.scratch);
+                reinterpret_cast<T*>(ixs + ntasks)[task] = best;
+                ixs[task] = bi;
+            }
+        }
+    }
+}
+
+template <int CD, bool MAX>
+__global__ void k_argext_top(RedDesc d) {
+    typedef ArgPol<CD, MAX> P;
+    typedef typename DT<CD>::T T;
+    const int64_t nseg = (int64_t)1 << d.K;
+    const int64_t ntasks = d.nout * nseg;
+    for (int64_t o = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; o < d.nout; o += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t* ix = reinterpret_cast<const int64_t*>(d.scratch) + o * nseg;
+        const T* v = reinterpret_cast<const T*>(reinterpret_cast<const int64_t*>(d.scratch) + ntasks) + o * nseg;
+        T best{};
+        int64_t bi = -1;
+        for (int64_t s = 0; s < nseg; ++s) {
+            if (P::takes(v[s], ix[s], best, bi)) { best = v[s]; bi = ix[s]; }
+        }
+        int64_t in_off, out_off;
+        kept_offsets(d, o, &in_off, &out_off);
+        ((int64_t*)d.o)[out_off] = bi < 0 ? 0 : bi;
+    }
+}
+
+// Column-order argext: one output per thread, sequential over the axis.
+template <int CD, bool MAX>
+__global__ void __launch_bounds__(RED_THREADS) k_argext_col(RedDesc d) {
+    typedef ArgPol<CD, MAX> P;
+    typedef typename DT<CD>::T T;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t o = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; o < d.nout; o += stride) {
+        int64_t base, out_off;
+        kept_offsets(d, o, &base, &out_off);
+        const T* p = (const T*)d.a + base;
+        T best = p[0];
+        int64_t bi = 0;
+        int64_t i = 1;
+        constexpr int U = 8;
+        for (; i + U <= d.w; i += U) {
+            T x[U];
+#pragma unroll
+            for (int u = 0; u < U; ++u) x[u] = p[(i + u) * d.ws];
+#pragma unroll
+            for (int u = 0; u < U; ++u) if (P::better(x[u], best)) { best = x[u]; bi = i + u; }
+        }
+        for (; i < d.w; ++i) {
+            T x = p[i * d.ws];
+            if (P::better(x, best)) { best = x; bi = i; }
+        }
+        ((int64_t*)d.o)[out_off] = bi;
+    }
+}
+
+// Launchers (ionp_reduce.cu)
+cudaError_t launch_reduce_row(const RedDesc& d, int tpr, size_t smem, int grid, cudaStream_t s);
+cudaError_t launch_reduce_row_top(const RedDesc& d, cudaStream_t s);
+cudaError_t launch_reduce_col(const RedDesc& d, cudaStream_t s);
+cudaError_t launch_reduce_gen(const RedDesc& d, cudaStream_t s);
+cudaError_t launch_reduce_masked(const RedDesc& d, cudaStream_t s);
+cudaError_t launch_argext(const RedDesc& d, int is_max, int mode, int tpr, cudaStream_t s);
+bool reduce_row_supported(int op, int cd);
+
+}  // namespace ionp

@@ -1,0 +1,57 @@
+// Row (tree) reduction launch templates, included by the per-op-group
+// translation units ionp_reduce_row_*.cu.
+#pragma once
+#include "ionp_reduce_launch.cuh"
+
+namespace ionp {
+
+constexpr bool red_castld_ok(int op, int cd) { return (op == OP_ADD || op == OP_MULTIPLY) && (cd == DT_I64 || cd == DT_U64); }
+
+template <int OP, int CD, bool C>
+static cudaError_t row_t2(const RedDesc& d, int tpr, size_t smem, int grid, cudaStream_t s) {
+    switch (tpr) {
+        case 1: k_red_row<OP, CD, 1, C><<<grid, RED_THREADS, smem, s>>>(d); break;
+        case 8: k_red_row<OP, CD, 8, C><<<grid, RED_THREADS, smem, s>>>(d); break;
+        case 32: k_red_row<OP, CD, 32, C><<<grid, RED_THREADS, smem, s>>>(d); break;
+        default: {
+            auto k = k_red_row<OP, CD, 256, C>;
+            if (smem > 48 * 1024) cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+            k<<<grid, RED_THREADS, smem, s>>>(d);
+        } break;
+    }
+    count_launch();
+    return cudaGetLastError();
+}
+
+template <int OP, int CD>
+static cudaError_t row_top_t(const RedDesc& d, cudaStream_t s) {
+    typedef typename RPol<OP, CD>::A A;
+    size_t smem = ((size_t)1 << d.K) * sizeof(A);
+    int grid = (int)(d.nout < 148 * 8 ? d.nout : 148 * 8);
+    auto k = k_red_row_top<OP, CD>;
+    if (smem > 48 * 1024) cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k<<<grid, RED_THREADS, smem, s>>>(d);
+    count_launch();
+    return cudaGetLastError();
+}
+
+template <int OPV>
+static cudaError_t row_op(const RedDesc& d, int tpr, size_t smem, int grid, cudaStream_t s, bool top) {
+    const bool castld = d.adt != d.cd;
+#define IONP_DTCASE(D)                                                                  \
+    case D:                                                                             \
+        if constexpr (red_row_valid(OPV, D)) {                                          \
+            if (top) return row_top_t<OPV, D>(d, s);                                    \
+            if constexpr (red_castld_ok(OPV, D)) {                                      \
+                if (castld) return row_t2<OPV, D, true>(d, tpr, smem, grid, s);         \
+            }                                                                           \
+            if (castld) return cudaErrorInvalidValue;                                   \
+            return row_t2<OPV, D, false>(d, tpr, smem, grid, s);                        \
+        }                                                                               \
+        break;
+    switch (d.cd) { IONP_DTS(IONP_DTCASE) }
+#undef IONP_DTCASE
+    return cudaErrorInvalidValue;
+}
+
+}  // namespace ionp

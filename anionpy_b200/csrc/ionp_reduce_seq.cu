@@ -1,0 +1,60 @@
+// Sequential (column) reduction kernels and the general wide x narrow kernel.
+#include "ionp_reduce_row_impl.cuh"
+
+namespace ionp {
+
+static int seq_grid(int64_t nout, int threads) {
+    int64_t g = (nout + threads - 1) / threads;
+    if (g < 1) g = 1;
+    if (g > 148 * 16) g = 148 * 16;
+    return (int)g;
+}
+
+template <int OPV>
+static cudaError_t col_op(const RedDesc& d, cudaStream_t s) {
+    const bool castld = d.adt != d.cd;
+    const int grid = seq_grid(d.nout, RED_THREADS);
+#define IONP_DTCASE(D)                                                                          \
+    case D:                                                                                     \
+        if constexpr (red_any_valid(OPV, D)) {                                                  \
+            if constexpr (red_castld_ok(OPV, D)) {                                              \
+                if (castld) { k_red_col<OPV, D, true><<<grid, RED_THREADS, 0, s>>>(d); count_launch(); return cudaGetLastError(); } \
+            }                                                                                   \
+            if (castld) return cudaErrorInvalidValue;                                           \
+            k_red_col<OPV, D, false><<<grid, RED_THREADS, 0, s>>>(d);                           \
+            count_launch();                                                                     \
+            return cudaGetLastError();                                                          \
+        }                                                                                       \
+        break;
+    switch (d.cd) { IONP_DTS(IONP_DTCASE) }
+#undef IONP_DTCASE
+    return cudaErrorInvalidValue;
+}
+
+cudaError_t launch_reduce_col(const RedDesc& d, cudaStream_t s) {
+#define IONP_OPCASE(OP) case OP: return col_op<OP>(d, s);
+    switch (d.op) { IONP_RED_OPS(IONP_OPCASE) }
+#undef IONP_OPCASE
+    return cudaErrorInvalidValue;
+}
+
+cudaError_t launch_reduce_gen(const RedDesc& d, cudaStream_t s) {
+    int grid = seq_grid(d.nout, 128);
+    switch (d.cd) {
+        case DT_F32: if (d.op == OP_ADD) { k_red_gen<OP_ADD, DT_F32><<<grid, 128, 0, s>>>(d); count_launch(); return cudaGetLastError(); } break;
+        case DT_F64: if (d.op == OP_ADD) { k_red_gen<OP_ADD, DT_F64><<<grid, 128, 0, s>>>(d); count_launch(); return cudaGetLastError(); } break;
+        case DT_F16:
+            switch (d.op) {
+                case OP_ADD: k_red_gen<OP_ADD, DT_F16><<<grid, 128, 0, s>>>(d); break;
+                case OP_MULTIPLY: k_red_gen<OP_MULTIPLY, DT_F16><<<grid, 128, 0, s>>>(d); break;
+                case OP_SUBTRACT: k_red_gen<OP_SUBTRACT, DT_F16><<<grid, 128, 0, s>>>(d); break;
+                case OP_DIVIDE: k_red_gen<OP_DIVIDE, DT_F16><<<grid, 128, 0, s>>>(d); break;
+                default: return cudaErrorInvalidValue;
+            }
+            count_launch();
+            return cudaGetLastError();
+    }
+    return cudaErrorInvalidValue;
+}
+
+}  // namespace ionp

@@ -1,0 +1,481 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 ufunc engine on the large element-wise sweep.
+
+Workload (one step = one pass over the whole sweep, 2^28 elements per
+operand): binary add, multiply, maximum, floor_divide, remainder and
+bitwise_and on int32/int64 (uniform over the full range, 1% zero divisors),
+the same arithmetic ufuncs on float32/float64 (N(0,1) with 0.1% NaN, 0.1%
++-inf, 0.1% signed zeros), unary exp (U[-100,100]) / log (U(0,1e6]) / sin
+(10*N(0,1)) on float32/float64; every case contiguous, on a transposed
+(16384, 16384) view and on a step-2 slice of a 2^29 base. Inputs are seeded
+synthetic data resident in HBM (1-8 GiB per operand, far larger than the
+126 MB L2, so no flush is needed between steps).
+
+Prints one JSON line (rank 0). --impl reference times the CPU restatement of
+the reference's engine on the host cores instead.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "ufunc+reduce GB/s (% HBM peak), bit-exact; mixed-stream calls/s vs per-launch"
+N_ELEM = 1 << 28
+SIDE = 16384
+BIN_OPS_INT = ["add", "multiply", "maximum", "floor_divide", "remainder", "bitwise_and"]
+BIN_OPS_FLT = ["add", "multiply", "maximum", "floor_divide", "remainder"]
+UN_OPS = ["exp", "log", "sin"]
+DTYPES = ["int32", "int64", "float32", "float64"]
+LAYOUTS = ["contig", "transposed", "step2"]
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+# ---------------------------------------------------------------------------
+# synthetic inputs
+# ---------------------------------------------------------------------------
+def gen_block(kind, dt, n, rng):
+    dt = np.dtype(dt)
+    if kind == "int":
+        info = np.iinfo(dt)
+        return rng.integers(info.min, info.max, n, dtype=dt, endpoint=True)
+    if kind == "divisor":
+        info = np.iinfo(dt)
+        x = rng.integers(info.min, info.max, n, dtype=dt, endpoint=True)
+        x[rng.random(n) < 0.01] = 0
+        return x
+    if kind == "float":
+        x = rng.standard_normal(n).astype(dt)
+        u = rng.random(n)
+        x[u < 0.001] = np.nan
+        x[(u >= 0.001) & (u < 0.0015)] = np.inf
+        x[(u >= 0.0015) & (u < 0.002)] = -np.inf
+        x[(u >= 0.002) & (u < 0.0025)] = 0.0
+        x[(u >= 0.0025) & (u < 0.003)] = -0.0
+        return x
+    if kind == "exp":
+        return rng.uniform(-100, 100, n).astype(dt)
+    if kind == "log":
+        return (1e6 * (1.0 - rng.random(n))).astype(dt)
+    if kind == "sin":
+        return (rng.standard_normal(n) * 10).astype(dt)
+    raise ValueError(kind)
+
+
+def device_fill(ap, L, kind, dt, n, seed, block=1 << 24):
+    """A device array of n values: one seeded host block, tiled on device."""
+    rng = np.random.default_rng(seed)
+    blk = gen_block(kind, dt, min(block, n), rng)
+    d = ap.empty((n,), dt)
+    nb = blk.nbytes
+    tmp = ap.from_numpy(blk)
+    off = 0
+    total = n * blk.itemsize
+    while off < total:
+        c = min(nb, total - off)
+        L.ionp_memcpy(d.data_ptr + off, tmp.data_ptr, c, 2, None)
+        off += c
+    L.ionp_stream_synchronize(None)
+    return d, blk
+
+
+def build_cases(ap, L, n):
+    """Case list: (name, op, dtype, layout, operands(list of device arrays), out bytes, in bytes)."""
+    cases = []
+    side = int(round(n ** 0.5))
+    bufs = {}
+    for dt in DTYPES:
+        isz = np.dtype(dt).itemsize
+        isint = dt.startswith("int")
+        a_base, _ = device_fill(ap, L, "int" if isint else "float", dt, 2 * n, 1000 + DTYPES.index(dt))
+        b_base, _ = device_fill(ap, L, "divisor" if isint else "float", dt, 2 * n, 2000 + DTYPES.index(dt))
+        bufs[dt] = (a_base, b_base)
+        views = {
+            "contig": (a_base[:n], b_base[:n]),
+            "transposed": (a_base[:n].reshape(side, side).T, b_base[n: 2 * n].reshape(side, side)),
+            "step2": (a_base[::2], b_base[::2]),
+        }
+        for op in (BIN_OPS_INT if isint else BIN_OPS_FLT):
+            for lay in LAYOUTS:
+                x, y = views[lay]
+                cases.append((f"{op}/{dt}/{lay}", op, dt, lay, [x, y], n * isz, 2 * n * isz))
+        if not isint:
+            for fn in UN_OPS:
+                base, _ = device_fill(ap, L, fn, dt, 2 * n, 3000 + UN_OPS.index(fn) + 10 * DTYPES.index(dt))
+                bufs[(dt, fn)] = base
+                uv = {"contig": base[:n], "transposed": base[:n].reshape(side, side).T, "step2": base[::2]}
+                for lay in LAYOUTS:
+                    cases.append((f"{fn}/{dt}/{lay}", fn, dt, lay, [uv[lay]], n * isz, n * isz))
+    return cases, bufs
+
+
+def sample(x, stride=4099):
+    """Every stride-th element (C order) of a device array, copied to host."""
+    flat = x if x.ndim == 1 else x.copy().reshape(-1)
+    return flat[::stride].get()
+
+
+def run_case(ap, case, outs):
+    name, op, dt, lay, operands, _, _ = case
+    key = (dt, lay, len(operands))
+    out = outs.get(key)
+    uf = getattr(ap, op)
+    if out is None:
+        out = uf(*operands)
+        outs[key] = out
+        return out
+    return uf(*operands, out=out)
+
+
+# ---------------------------------------------------------------------------
+# clocks sampled during the timed region
+# ---------------------------------------------------------------------------
+class Clocks:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        res = {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        if not self.proc:
+            return res
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        rows = []
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 9:
+                rows.append(parts)
+        os.unlink(self.path)
+        if not rows:
+            return res
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        res["samples"] = len(rows)
+        res["sm_mhz"] = statistics.median(sm) if sm else None
+        res["sm_max_mhz"] = float(rows[0][2]) if rows[0][2].replace(".", "").isdigit() else None
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for r in rows:
+            for i, nm in enumerate(names):
+                if r[5 + i].lower() == "active":
+                    reasons.add(nm)
+        res["reasons"] = sorted(reasons)
+        res["power_w_max"] = max((float(r[3]) for r in rows if r[3].replace(".", "").isdigit()), default=None)
+        return res
+
+
+# ---------------------------------------------------------------------------
+# CPU side: the oracle (the restatement of the reference's engine)
+# ---------------------------------------------------------------------------
+def cpu_sample_cases(n):
+    rng = np.random.default_rng(99)
+    out = []
+    for dt in DTYPES:
+        isint = dt.startswith("int")
+        a = gen_block("int" if isint else "float", dt, n, rng)
+        b = gen_block("divisor" if isint else "float", dt, n, rng)
+        for op in (BIN_OPS_INT if isint else BIN_OPS_FLT):
+            out.append((op, [a, b], 3 * n * np.dtype(dt).itemsize))
+        if not isint:
+            for fn in UN_OPS:
+                out.append((fn, [gen_block(fn, dt, n, rng)], 2 * n * np.dtype(dt).itemsize))
+    return out
+
+
+def time_oracle(cases, threads):
+    from concurrent.futures import ThreadPoolExecutor
+    from oracle import oracle as O
+    O.lib()
+    total_bytes = 0
+    t0 = time.perf_counter()
+    with ThreadPoolExecutor(max_workers=threads) as ex:
+        for op, ops, nbytes in cases:
+            n = ops[0].size
+            chunks = [(i * n // threads, (i + 1) * n // threads) for i in range(threads)]
+            if len(ops) == 2:
+                fs = [ex.submit(O.binary, op, ops[0][lo:hi], ops[1][lo:hi]) for lo, hi in chunks]
+            else:
+                fs = [ex.submit(O.unary, op, ops[0][lo:hi]) for lo, hi in chunks]
+            for f in fs:
+                f.result()
+            total_bytes += nbytes
+    dt = time.perf_counter() - t0
+    return total_bytes / dt / 1e9, dt
+
+
+def reference_arm(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    threads = os.cpu_count() or 1
+    n = 1 << 21
+    cases = cpu_sample_cases(n)
+    for _ in range(args.warmup):
+        time_oracle(cases[:2], threads)
+    vals = []
+    for _ in range(args.steps):
+        v, _ = time_oracle(cases, threads)
+        vals.append(v)
+    value = statistics.median(vals)
+    sample = f"{len(cases)} contiguous sweep cases x {n} elements (2^21 of 2^28) per step, split over {threads} threads"
+    line = {
+        "metric": METRIC, "value": round(value, 3), "unit": "GB/s", "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "mixed(int32,int64,f32,f64)", "data": "synthetic",
+        "config": {"workload": "large element-wise sweep, contiguous cases (bounded CPU sample)", "elements": n},
+        "impl": "reference",
+        "cpu_baseline": {"value": round(value, 3), "unit": "GB/s", "cores": threads, "kind": "port", "sample": sample},
+        "e2e": {"value": round(value, 3), "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------
+# GPU arm
+# ---------------------------------------------------------------------------
+def main():
+    ap_ = argparse.ArgumentParser()
+    ap_.add_argument("--gpus", type=int, default=1)
+    ap_.add_argument("--steps", type=int, default=5)
+    ap_.add_argument("--warmup", type=int, default=3)
+    ap_.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap_.add_argument("--elements", type=int, default=N_ELEM, help="elements per operand (default 2^28)")
+    ap_.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline leg")
+    ap_.add_argument("--no-e2e", action="store_true")
+    args = ap_.parse_args()
+    if args.impl == "reference":
+        return reference_arm(args)
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+
+    import anionpy_b200 as ap
+    from anionpy_b200 import _lib
+    L = _lib.lib()
+    _lib.check(L.ionp_set_device(local))
+    n = args.elements
+    side = int(round(n ** 0.5))
+    assert side * side == n, "elements must be a perfect square"
+    hbm_peak, peak_kind = peaks()
+
+    cases, bufs = build_cases(ap, L, n)
+    outs = {}
+    ev = [ctypes.c_void_p() for _ in range(len(cases) + 1)]
+    for e in ev:
+        _lib.check(L.ionp_event_create(ctypes.byref(e)))
+    t_start, t_stop = ctypes.c_void_p(), ctypes.c_void_p()
+    L.ionp_event_create(ctypes.byref(t_start))
+    L.ionp_event_create(ctypes.byref(t_stop))
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    # warm-up
+    for _ in range(max(args.warmup, 1)):
+        for c in cases:
+            run_case(ap, c, outs)
+    L.ionp_device_synchronize()
+
+    clocks = Clocks(local)
+    clocks.start()
+    barrier()
+    L.ionp_device_synchronize()
+    launches0 = _lib.launch_count()
+    per_case = np.zeros(len(cases))
+    L.ionp_event_record(t_start, None)
+    for _ in range(args.steps):
+        L.ionp_event_record(ev[0], None)
+        for i, c in enumerate(cases):
+            run_case(ap, c, outs)
+            L.ionp_event_record(ev[i + 1], None)
+        L.ionp_device_synchronize()
+        for i in range(len(cases)):
+            ms = ctypes.c_float()
+            L.ionp_event_elapsed_ms(ev[i], ev[i + 1], ctypes.byref(ms))
+            per_case[i] += ms.value
+    L.ionp_event_record(t_stop, None)
+    L.ionp_device_synchronize()
+    barrier()
+    launches = _lib.launch_count() - launches0
+    clk = clocks.stop()
+    tot = ctypes.c_float()
+    L.ionp_event_elapsed_ms(t_start, t_stop, ctypes.byref(tot))
+    total_ms = tot.value
+    if dist is not None:
+        import torch
+        t = torch.tensor([total_ms], device=f"cuda:{local}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    step_bytes = sum(c[5] + c[6] for c in cases)
+    value = step_bytes * args.steps * world / (total_ms / 1e3) / 1e9
+
+    # per-case achieved bandwidth and the dominant kernel's roofline
+    per_case /= args.steps
+    rows = []
+    for c, ms in zip(cases, per_case):
+        gbs = (c[5] + c[6]) / (ms / 1e3) / 1e9
+        rows.append({"case": c[0], "ms": round(float(ms), 4), "GB/s": round(gbs, 1), "frac": round(gbs / hbm_peak, 3)})
+    dom = int(np.argmax(per_case))
+    head = [r for r in rows if r["case"] == "add/float32/contig"][0]
+
+    # parity on a sample of every case (full-size inputs, oracle on a stride)
+    mismatches = 0
+    checked = 0
+    if rank == 0:
+        from oracle import oracle as O
+        for c in cases:
+            name, op, dt, lay, operands, _, _ = c
+            out = run_case(ap, c, outs)
+            if op in UN_OPS:
+                continue  # transcendentals: ULP-checked in tests/, not bitwise here
+            hosts = [sample(o) for o in operands]
+            want = O.binary(op, *hosts)[0]
+            got = sample(out)
+            mismatches += int(got.tobytes() != want.tobytes())
+            checked += 1
+
+    # end-to-end through the public API with pinned host buffers
+    e2e = None
+    if not args.no_e2e and rank == 0:
+        e2e = end_to_end(ap, L, n, min(args.steps, 2))
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        sample_n = 1 << 22
+        v, secs = time_oracle(cpu_sample_cases(sample_n), 1)
+        cpu = {"value": round(v, 3), "unit": "GB/s", "cores": 1, "kind": "port",
+               "sample": f"the {len(cpu_sample_cases(16))} contiguous sweep cases at {sample_n} elements each (2^22 of 2^28), "
+                         f"single thread, {secs:.1f} s of CPU work"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": round(value, 2), "unit": "GB/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(total_ms / args.steps, 3), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "mixed(int32,int64,f32,f64)", "data": "synthetic",
+            "config": {"workload": "large element-wise sweep: 6 binary ufuncs x int32/int64, 5 x float32/float64, "
+                                   "exp/log/sin x float32/float64; contiguous, transposed (16384,16384) view, step-2 slice",
+                       "elements_per_operand": n, "cases": len(cases), "l2": "inputs 1-8 GiB per operand > 126 MB L2, no flush",
+                       "parallelism": f"replicas x{world}"},
+            "roofline": {"bound": "hbm", "kernel": rows[dom]["case"], "achieved": rows[dom]["GB/s"], "peak": hbm_peak,
+                         "unit": "GB/s", "frac": rows[dom]["frac"], "traffic": None, "peak_kind": peak_kind,
+                         "headline_add_f32_contig": head},
+            "cpu_baseline": cpu,
+            "e2e": e2e,
+            "gpu_launches": int(launches),
+            "clocks": clk,
+            "parity": {"cases_checked": checked, "cases_with_mismatch": mismatches, "sample_stride": 4099},
+            "cases": rows,
+        }
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+def end_to_end(ap, L, n, steps):
+    """GB/s of the contiguous cases through the public API, inputs copied from
+    pinned host buffers and results read back inside the timed region."""
+    from anionpy_b200 import _lib
+    itemmax = 8
+    hp = [ctypes.c_void_p() for _ in range(3)]
+    for h in hp:
+        _lib.check(L.ionp_host_alloc(ctypes.byref(h), n * itemmax))
+    rng = np.random.default_rng(5)
+    todo = []
+    for dt in DTYPES:
+        isint = dt.startswith("int")
+        for op in (BIN_OPS_INT if isint else BIN_OPS_FLT):
+            todo.append((op, dt, 2))
+        if not isint:
+            for fn in UN_OPS:
+                todo.append((fn, dt, 1))
+    dev = {}
+    for dt in DTYPES:
+        dev[dt] = (ap.empty((n,), dt), ap.empty((n,), dt), ap.empty((n,), dt))
+    # host data (one block tiled)
+    for i, h in enumerate(hp[:2]):
+        blk = gen_block("float", np.float64, 1 << 22, rng).view(np.uint8)
+        arr = np.ctypeslib.as_array((ctypes.c_uint8 * (n * itemmax)).from_address(h.value))
+        for off in range(0, arr.size, blk.size):
+            arr[off: off + blk.size] = blk[: arr.size - off]
+    e0, e1 = ctypes.c_void_p(), ctypes.c_void_p()
+    L.ionp_event_create(ctypes.byref(e0))
+    L.ionp_event_create(ctypes.byref(e1))
+    h2d = d2h = 0
+    nbytes = 0
+    L.ionp_device_synchronize()
+    L.ionp_event_record(e0, None)
+    for _ in range(steps):
+        for op, dt, k in todo:
+            isz = np.dtype(dt).itemsize
+            a, b, o = dev[dt]
+            L.ionp_memcpy(a.data_ptr, hp[0], n * isz, 0, None)
+            h2d += n * isz
+            if k == 2:
+                L.ionp_memcpy(b.data_ptr, hp[1], n * isz, 0, None)
+                h2d += n * isz
+                getattr(ap, op)(a, b, out=o)
+            else:
+                getattr(ap, op)(a, out=o)
+            L.ionp_memcpy(hp[2], o.data_ptr, n * isz, 1, None)
+            d2h += n * isz
+            nbytes += (k + 1) * n * isz
+    L.ionp_event_record(e1, None)
+    ms = ctypes.c_float()
+    L.ionp_event_elapsed_ms(e0, e1, ctypes.byref(ms))
+    for h in hp:
+        L.ionp_host_free(h)
+    return {"value": round(nbytes / (ms.value / 1e3) / 1e9, 3), "unit": "GB/s",
+            "h2d_bytes_per_step": h2d // steps, "d2h_bytes_per_step": d2h // steps}
+
+
+if __name__ == "__main__":
+    import anionpy_b200 as _ap
+    if "--impl" in sys.argv and "reference" in sys.argv:
+        main()
+    else:
+        with _ap.errstate(all="ignore"):
+            main()

@@ -1,0 +1,184 @@
+/*
+ * ionp_cuda.h -- C ABI of the B200 ufunc engine (libionp_cuda.so).
+ *
+ * This is the seam the reference's Rust engine API occupies:
+ * ionp_core::ufunc::{binary_op, unary_op, math_unary_op, math_binary_op,
+ * reduce_axis, argext, write_out} over `&NdArray`, returning
+ * `Result<NdArray, IonpError>` (Son0fSun/anionpy, ionp-core/src/ufunc.rs).
+ * Arrays are plain descriptors over device memory; no C++ or torch types
+ * cross this boundary. Every entry point returns an int32 status
+ * (IONP_OK = 0); the message of the last failure on the calling thread is
+ * available from ionp_last_error_message().
+ *
+ * Conventions (the reference's, ionp-core/src/shape.rs:1-5 and
+ * ionp-core/src/array.rs:24-40):
+ *   - strides and offsets are in ELEMENTS, not bytes;
+ *   - `data` is the base of the allocation, `offset` the first element;
+ *   - dtype codes follow ionp-core/src/dtype.rs:14 (complex excluded).
+ * The caller owns every buffer; outputs are allocated by the caller after
+ * host-side planning (shape, dtype and layout from the query functions).
+ */
+#ifndef IONP_CUDA_H
+#define IONP_CUDA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define IONP_MAX_DIMS 32
+
+/* dtype codes (ionp-core/src/dtype.rs:14-28) */
+enum {
+    IONP_BOOL = 0, IONP_INT8, IONP_INT16, IONP_INT32, IONP_INT64,
+    IONP_UINT8, IONP_UINT16, IONP_UINT32, IONP_UINT64,
+    IONP_FLOAT16, IONP_FLOAT32, IONP_FLOAT64
+};
+
+/* op codes: BinaryOp (ufunc.rs:43-65) in declaration order, then the
+ * MathBinaryOp / UnaryOp / MathUnaryOp members this engine implements. */
+enum {
+    IONP_ADD = 0, IONP_SUBTRACT, IONP_MULTIPLY, IONP_DIVIDE, IONP_MAXIMUM, IONP_MINIMUM,
+    IONP_GREATER, IONP_GREATER_EQUAL, IONP_LESS, IONP_LESS_EQUAL, IONP_EQUAL, IONP_NOT_EQUAL,
+    IONP_LOGICAL_AND, IONP_LOGICAL_OR, IONP_LOGICAL_XOR,
+    IONP_BITWISE_AND, IONP_BITWISE_OR, IONP_BITWISE_XOR,
+    IONP_FLOOR_DIVIDE, IONP_LEFT_SHIFT, IONP_RIGHT_SHIFT,
+    IONP_REMAINDER = 32, IONP_FMOD = 33,
+    IONP_NEGATIVE = 64, IONP_ABSOLUTE = 65, IONP_INVERT = 66, IONP_LOGICAL_NOT = 67,
+    IONP_SQRT = 80, IONP_EXP = 81, IONP_LOG = 82, IONP_SIN = 83
+};
+
+/* status codes: 1:1 with IonpError variants (ionp-core/src/error.rs:8-40),
+ * plus device-side failures. */
+enum {
+    IONP_OK = 0,
+    IONP_ERR_BROADCAST = 1,   /* IonpError::Broadcast  -> ValueError */
+    IONP_ERR_TYPE = 2,        /* IonpError::Type       -> TypeError */
+    IONP_ERR_VALUE = 3,       /* IonpError::Value      -> ValueError */
+    IONP_ERR_NO_LOOP = 4,     /* IonpError::NoUfuncLoop -> UFuncTypeError */
+    IONP_ERR_AXIS = 5,        /* IonpError::AxisError  -> AxisError */
+    IONP_ERR_CUDA = 6,        /* a CUDA runtime call failed */
+    IONP_ERR_TIMEOUT = 7,     /* a bounded device-side wait ran out */
+    IONP_ERR_OOM = 8,         /* device allocation failed */
+    IONP_ERR_UNSUPPORTED = 9, /* dtype/op outside this engine (e.g. complex) */
+    IONP_ERR_INVALID = 10     /* malformed descriptor or argument */
+};
+
+/* FPE category bits (ionp-core/src/fpe.rs:43-48) */
+enum { IONP_FPE_DIVIDE = 1, IONP_FPE_OVER = 2, IONP_FPE_UNDER = 4, IONP_FPE_INVALID = 8 };
+
+/* casting rules for ionp_can_cast (ionp-core/src/dtype.rs:823) */
+enum { IONP_CAST_NO = 0, IONP_CAST_EQUIV = 1, IONP_CAST_SAFE = 2, IONP_CAST_SAME_KIND = 3, IONP_CAST_UNSAFE = 4 };
+
+typedef struct IonpArr {
+    int32_t dtype;
+    int32_t ndim;
+    int64_t shape[IONP_MAX_DIMS];
+    int64_t strides[IONP_MAX_DIMS]; /* elements */
+    int64_t offset;                 /* elements */
+    void* data;                     /* device pointer: base of the allocation */
+} IonpArr;
+
+typedef void* IonpStream; /* a cudaStream_t; NULL = the legacy default stream */
+
+/* ---------------------------------------------------------------- queries */
+/* promote_dtype (ionp-core/src/dtype.rs:297) */
+int32_t ionp_promote(int32_t a, int32_t b, int32_t* out);
+/* binary_out_dtype (ufunc.rs:1101) / math_binary_out_dtype (ufunc.rs:1785) */
+int32_t ionp_binary_out_dtype(int32_t op, int32_t a, int32_t b, int32_t* out);
+/* unary_out_dtype (ufunc.rs:1608) / math_unary_out_dtype (ufunc.rs:1682) */
+int32_t ionp_unary_out_dtype(int32_t op, int32_t a, int32_t* out);
+/* reduce_family_compute_dtype (ufunc.rs:2080) + supports_reduce_family (ufunc.rs:106) */
+int32_t ionp_reduce_compute_dtype(int32_t op, int32_t a, int32_t* out);
+/* can_cast (ionp-core/src/dtype.rs:823); *out = 0/1 */
+int32_t ionp_can_cast(int32_t from, int32_t to, int32_t rule, int32_t* out);
+/* One scalar converted with the reference's cast rules (Buffer::cast_to,
+ * ionp-core/src/buffer.rs:64-330): used for initial= values. Host memory. */
+int32_t ionp_cast_scalar(const void* src, int32_t src_dtype, void* dst, int32_t dst_dtype);
+/* Element strides of the order='K' result of a call over `nops` operands
+ * (ionp-py/src/lib.rs:1290-1330, ionp-core/src/array.rs:1153). */
+int32_t ionp_order_k_strides(int32_t nops, const IonpArr* const* ops, int32_t ndim, const int64_t* out_shape,
+                             int64_t* out_strides);
+/* Shape and element strides of a reduction result
+ * (ionp-core/src/array.rs:845-930, relayout_for_reduction). */
+int32_t ionp_reduce_layout(const IonpArr* a, const int32_t* axes, int32_t naxes, int32_t keepdims,
+                           int32_t* out_ndim, int64_t* out_shape, int64_t* out_strides);
+
+/* ---------------------------------------------------------------- compute */
+/* Element-wise binary ufunc: binary_op (ufunc.rs:3628) or math_binary_op
+ * (ufunc.rs:5733) followed by write_out (ufunc.rs:10112).
+ *   out   : caller-allocated, shape = broadcast(a, b) or wider (out= may
+ *           broadcast up), any strides; its dtype may differ from the loop
+ *           dtype (the value is cast on store, as write_into_out_ufunc does).
+ *   where : NULL, or a bool mask broadcastable to out (masked store).
+ *   fpe   : NULL, or a host word that receives the OR of IONP_FPE_* bits of
+ *           the reference's post-hoc detector for this op
+ *           (ionp-py/src/lib.rs:9077-9138); non-NULL makes the call wait for
+ *           the stream. */
+int32_t ionp_binary(int32_t op, const IonpArr* a, const IonpArr* b, IonpArr* out, const IonpArr* where,
+                    uint32_t* fpe, IonpStream stream);
+/* Element-wise unary ufunc: unary_op (ufunc.rs:3824) / math_unary_op
+ * (ufunc.rs:4606). Same out/where/fpe conventions as ionp_binary. */
+int32_t ionp_unary(int32_t op, const IonpArr* a, IonpArr* out, const IonpArr* where, uint32_t* fpe,
+                   IonpStream stream);
+/* Element-wise dtype conversion/copy of `a` into `out` (same shape, any
+ * strides): Buffer::cast_to (ionp-core/src/buffer.rs:210). */
+int32_t ionp_cast(const IonpArr* a, IonpArr* out, IonpStream stream);
+/* ufunc.reduce: reduce_axis (ufunc.rs:7634).
+ *   axes          : normalized, sorted, unique (normalize_reduce_axes, ufunc.rs:7551)
+ *   compute_dtype : -1 = reduce_family_compute_dtype, else the dtype= override
+ *   initial       : NULL, or a HOST pointer to one value of the compute dtype
+ *   where         : NULL, or a mask broadcastable to a (any dtype, cast to bool)
+ *   out           : caller-allocated, the kept shape (keepdims or not), any
+ *                   strides; value cast on store when its dtype differs. */
+int32_t ionp_reduce(int32_t op, const IonpArr* a, const int32_t* axes, int32_t naxes, int32_t keepdims,
+                    int32_t compute_dtype, const void* initial, const IonpArr* where, IonpArr* out,
+                    IonpStream stream);
+/* argmin (is_max=0) / argmax (is_max=1): argext (ufunc.rs:8131) behind
+ * do_argext (ionp-py/src/reductions.rs:1198). axis = -1 means the flattened
+ * C-order ravel (axis=None); out is int64 with the kept shape. */
+int32_t ionp_argext(int32_t is_max, const IonpArr* a, int32_t axis, int32_t keepdims, IonpArr* out,
+                    IonpStream stream);
+
+/* ---------------------------------------------------------------- memory */
+/* Caching device allocator (the device counterpart of Buffer's Vec<T>,
+ * ionp-core/src/buffer.rs:18): size-classed free lists, stream-ordered reuse. */
+int32_t ionp_alloc(void** ptr, size_t bytes, IonpStream stream);
+int32_t ionp_free(void* ptr, IonpStream stream);
+/* bytes: [0] in use, [1] cached (free), [2] peak in use, [3] cudaMalloc calls */
+int32_t ionp_alloc_stats(uint64_t* stats4);
+int32_t ionp_alloc_trim(void);
+
+/* ---------------------------------------------------------------- runtime */
+/* Thin runtime helpers so hosts need no CUDA bindings of their own. */
+enum { IONP_H2D = 0, IONP_D2H = 1, IONP_D2D = 2 };
+int32_t ionp_memcpy(void* dst, const void* src, size_t bytes, int32_t kind, IonpStream stream);
+int32_t ionp_stream_create(IonpStream* stream);
+int32_t ionp_stream_destroy(IonpStream stream);
+int32_t ionp_stream_synchronize(IonpStream stream);
+int32_t ionp_device_synchronize(void);
+/* pinned host memory (page-locked; fast, asynchronous copies) */
+int32_t ionp_host_alloc(void** ptr, size_t bytes);
+int32_t ionp_host_free(void* ptr);
+/* events for device-side timing on a stream */
+int32_t ionp_event_create(void** ev);
+int32_t ionp_event_destroy(void* ev);
+int32_t ionp_event_record(void* ev, IonpStream stream);
+int32_t ionp_event_elapsed_ms(void* start, void* stop, float* ms);
+/* select the CUDA device used by the calling host thread */
+int32_t ionp_set_device(int32_t device);
+/* device name / SM count / whether a device is present (count=0 if none) */
+int32_t ionp_device_info(int32_t* count, int32_t* sm_count, char* name, size_t len);
+
+/* ---------------------------------------------------------------- misc */
+/* Copies the last error message of the calling thread (NUL-terminated). */
+int32_t ionp_last_error_message(char* buf, size_t len);
+/* Number of kernels this library has launched since load (all streams). */
+uint64_t ionp_launch_count(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* IONP_CUDA_H */

@@ -1,0 +1,334 @@
+"""TEST INFRASTRUCTURE ONLY -- the parity oracle's Python face.
+
+ctypes wrapper over ``liboracle.so`` (``ionp_oracle.cpp``, a CPU restatement
+of anionpy's ufunc engine). Only ``tests/``, ``__graft_entry__.smoke()`` and
+the ``cpu_baseline`` leg of ``bench.py`` may import this module, and only to
+check or time the reference behaviour; the product never calls it.
+
+Besides the numeric calls it restates, in plain Python, the reference's
+metadata rules that decide result layout (these touch shapes and strides
+only):
+
+* ``multi_sorted_stride_perm`` / ``apply_ufunc_order`` -- order='K' output
+  layout of a ufunc call (ionp-core/src/array.rs:1153-1222,
+  ionp-py/src/lib.rs:1290-1330);
+* ``reduce_output_layout`` / ``relayout_for_reduction`` -- layout of a
+  reduction result (ionp-core/src/array.rs:845-930);
+* ``normalize_reduce_axes`` (ionp-core/src/ufunc.rs:7551-7632).
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "liboracle.so")
+
+# dtype codes in the order of ionp-core/src/dtype.rs:14
+NP_DTYPES = [np.bool_, np.int8, np.int16, np.int32, np.int64, np.uint8, np.uint16,
+             np.uint32, np.uint64, np.float16, np.float32, np.float64]
+CODE = {np.dtype(t): i for i, t in enumerate(NP_DTYPES)}
+
+OPS = {
+    "add": 0, "subtract": 1, "multiply": 2, "divide": 3, "maximum": 4, "minimum": 5,
+    "greater": 6, "greater_equal": 7, "less": 8, "less_equal": 9, "equal": 10, "not_equal": 11,
+    "logical_and": 12, "logical_or": 13, "logical_xor": 14,
+    "bitwise_and": 15, "bitwise_or": 16, "bitwise_xor": 17,
+    "floor_divide": 18, "left_shift": 19, "right_shift": 20,
+    "remainder": 32, "fmod": 33,
+    "negative": 64, "absolute": 65, "invert": 66, "logical_not": 67,
+    "sqrt": 80, "exp": 81, "log": 82, "sin": 83,
+}
+FPE_NAMES = {0: None, 1: "divide", 2: "over", 4: "under", 8: "invalid"}
+STATUS = {1: "broadcast", 2: "type", 3: "value", 4: "no_loop", 5: "axis", 9: "unsupported"}
+
+
+class OrArr(ctypes.Structure):
+    _fields_ = [("dtype", ctypes.c_int32), ("ndim", ctypes.c_int32),
+                ("shape", ctypes.c_int64 * 32), ("strides", ctypes.c_int64 * 32),
+                ("offset", ctypes.c_int64), ("data", ctypes.c_void_p)]
+
+
+class OracleError(Exception):
+    def __init__(self, status):
+        super().__init__(STATUS.get(status, status))
+        self.status = STATUS.get(status, status)
+
+
+def build():
+    """Compile liboracle.so from ionp_oracle.cpp (idempotent)."""
+    src = os.path.join(_HERE, "ionp_oracle.cpp")
+    if (not os.path.exists(_LIB_PATH)) or os.path.getmtime(_LIB_PATH) < os.path.getmtime(src):
+        subprocess.check_call(["make", "-s", "-C", _HERE])
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        build()
+        L = ctypes.CDLL(_LIB_PATH)
+        P = ctypes.POINTER(OrArr)
+        L.oracle_binary.argtypes = [ctypes.c_int, P, P, P, ctypes.POINTER(ctypes.c_int)]
+        L.oracle_unary.argtypes = [ctypes.c_int, P, P, ctypes.POINTER(ctypes.c_int)]
+        L.oracle_reduce.argtypes = [ctypes.c_int, P, ctypes.c_int, ctypes.POINTER(ctypes.c_int32),
+                                    ctypes.c_int, P, P, P]
+        L.oracle_argext.argtypes = [ctypes.c_int, P, ctypes.c_int, P]
+        L.oracle_cast.argtypes = [P, P]
+        L.oracle_pairwise_f64.argtypes = [ctypes.c_void_p, ctypes.c_int64]
+        L.oracle_pairwise_f64.restype = ctypes.c_double
+        _lib = L
+    return _lib
+
+
+def _desc(a: np.ndarray) -> OrArr:
+    d = OrArr()
+    d.dtype = CODE[a.dtype]
+    d.ndim = a.ndim
+    for i in range(a.ndim):
+        d.shape[i] = a.shape[i]
+        st = a.strides[i]
+        assert st % a.itemsize == 0
+        d.strides[i] = st // a.itemsize
+    d.offset = 0
+    d.data = a.ctypes.data if a.size else (np.zeros(1, a.dtype).ctypes.data)
+    return d
+
+
+def np_dtype(code: int):
+    return np.dtype(NP_DTYPES[code])
+
+
+def binary_out_dtype(op: str, da, db):
+    r = lib().oracle_binary_out_dtype(OPS[op], CODE[np.dtype(da)], CODE[np.dtype(db)])
+    if r < 0:
+        raise OracleError(-r)
+    return np_dtype(r)
+
+
+def unary_out_dtype(op: str, da):
+    r = lib().oracle_unary_out_dtype(OPS[op], CODE[np.dtype(da)])
+    if r < 0:
+        raise OracleError(-r)
+    return np_dtype(r)
+
+
+def reduce_compute_dtype(op: str, da):
+    r = lib().oracle_reduce_compute_dtype(OPS[op], CODE[np.dtype(da)])
+    if r < 0:
+        raise OracleError(-r)
+    return np_dtype(r)
+
+
+def binary(op: str, a: np.ndarray, b: np.ndarray):
+    """(C-order result, fpe category name or None) of ufunc `op`(a, b)."""
+    a = np.asarray(a)
+    b = np.asarray(b)
+    od = binary_out_dtype(op, a.dtype, b.dtype)
+    shape = np.broadcast_shapes(a.shape, b.shape)
+    out = np.empty(shape, od)
+    fpe = ctypes.c_int(0)
+    st = lib().oracle_binary(OPS[op], _desc(a), _desc(b), _desc(out), ctypes.byref(fpe))
+    if st:
+        raise OracleError(st)
+    return out, FPE_NAMES[fpe.value]
+
+
+def unary(op: str, a: np.ndarray):
+    a = np.asarray(a)
+    od = unary_out_dtype(op, a.dtype)
+    out = np.empty(a.shape, od)
+    fpe = ctypes.c_int(0)
+    st = lib().oracle_unary(OPS[op], _desc(a), _desc(out), ctypes.byref(fpe))
+    if st:
+        raise OracleError(st)
+    return out, FPE_NAMES[fpe.value]
+
+
+def cast(a: np.ndarray, dtype) -> np.ndarray:
+    out = np.empty(a.shape, dtype)
+    lib().oracle_cast(_desc(np.asarray(a)), _desc(out))
+    return out
+
+
+def normalize_reduce_axes(axis, ndim):
+    """normalize_reduce_axes (ionp-core/src/ufunc.rs:7551-7632)."""
+    if axis is None:
+        return list(range(ndim))
+    raw = list(axis) if isinstance(axis, (tuple, list)) else [axis]
+    out = []
+    for ax in raw:
+        norm = ax + max(ndim, 1) if ax < 0 else ax
+        if ndim == 0:
+            if norm != 0:
+                raise OracleError(5)
+        elif norm < 0 or norm >= ndim:
+            raise OracleError(5)
+        out.append(max(norm, 0))
+    if len(set(out)) != len(out):
+        raise OracleError(3)
+    return [] if ndim == 0 else sorted(out)
+
+
+def reduce(op: str, a: np.ndarray, axis=0, dtype=None, keepdims=False, initial=None, where=None):
+    """ufunc.reduce values (C-order over kept axes, keepdims re-inserted)."""
+    a = np.asarray(a)
+    axes = normalize_reduce_axes(axis, a.ndim)
+    cd = np.dtype(dtype) if dtype is not None else reduce_compute_dtype(op, a.dtype)
+    keep = [a.shape[i] for i in range(a.ndim) if i not in axes]
+    out = np.empty(max(int(np.prod(keep)), 1) if not keep else keep, cd)
+    if not keep:
+        out = np.empty((1,), cd)
+    ax = (ctypes.c_int32 * max(len(axes), 1))(*axes)
+    ini = _desc(np.asarray(initial)) if initial is not None else None
+    msk = None
+    if where is not None:
+        w = np.asarray(where)
+        msk = _desc(w)
+    st = lib().oracle_reduce(OPS[op], _desc(a), len(axes), ax, CODE[cd],
+                             ctypes.byref(ini) if ini is not None else None,
+                             ctypes.byref(msk) if msk is not None else None, _desc(out))
+    if st:
+        raise OracleError(st)
+    res = out.reshape(keep) if keep else out.reshape(())
+    if keepdims:
+        res = res.reshape([1 if i in axes else a.shape[i] for i in range(a.ndim)])
+    return res
+
+
+def argext(which: str, a: np.ndarray, axis=None, keepdims=False):
+    """argmin/argmax (ionp-py/src/reductions.rs:1198-1300, ufunc.rs:8131)."""
+    a = np.asarray(a)
+    ndim = a.ndim
+    if axis is None:
+        t = np.ascontiguousarray(a).reshape(-1)
+        ax = 0
+    else:
+        ax = axis + max(ndim, 1) if axis < 0 else axis
+        if ax < 0 or ax >= max(ndim, 1):
+            raise OracleError(5)
+        t = a
+    keep = [t.shape[i] for i in range(t.ndim) if i != ax]
+    out = np.empty(keep if keep else (1,), np.int64)
+    st = lib().oracle_argext(1 if which == "argmax" else 0, _desc(t), ax, _desc(out))
+    if st:
+        raise OracleError(st)
+    res = out.reshape(keep) if keep else out.reshape(())
+    if keepdims and t.ndim != 0:
+        res = res.reshape([1 if i == ax else t.shape[i] for i in range(t.ndim)])
+    if axis is None and keepdims and ndim != 1:
+        res = res.reshape([1] * ndim)
+    return res
+
+
+def pairwise_sum_f64(x: np.ndarray) -> float:
+    x = np.ascontiguousarray(x, np.float64)
+    return lib().oracle_pairwise_f64(x.ctypes.data, x.size)
+
+
+# ---------------------------------------------------------------------------
+# Layout rules (metadata only)
+# ---------------------------------------------------------------------------
+def c_strides(shape):
+    st, acc = [0] * len(shape), 1
+    for i in range(len(shape) - 1, -1, -1):
+        st[i] = acc
+        acc *= max(shape[i], 1)
+    return st
+
+
+def elem_strides(a: np.ndarray):
+    return [s // a.itemsize for s in a.strides]
+
+
+def multi_sorted_stride_perm(ndim, operands):
+    """ionp-core/src/array.rs:1153-1205 (operands: list of (shape, elem strides))."""
+    perm = list(range(ndim))
+    for i0 in range(1, ndim):
+        ax_j0 = perm[i0]
+        ipos = i0
+        i1 = i0
+        while i1 > 0:
+            i1 -= 1
+            ax_j1 = perm[i1]
+            ambig, shouldswap = True, False
+            for shape, strides in operands:
+                off = ndim - len(shape)
+                if ax_j0 < off or ax_j1 < off:
+                    continue
+                s0, s1 = shape[ax_j0 - off], shape[ax_j1 - off]
+                if s0 == 1 or s1 == 1:
+                    continue
+                st0, st1 = abs(strides[ax_j0 - off]), abs(strides[ax_j1 - off])
+                if st0 <= st1:
+                    shouldswap = False
+                elif ambig:
+                    shouldswap = True
+                ambig = False
+            if not ambig:
+                if shouldswap:
+                    ipos = i1
+                else:
+                    break
+        if ipos != i0:
+            perm[ipos + 1:i0 + 1] = perm[ipos:i0]
+        perm[ipos] = ax_j0
+    return perm
+
+
+def perm_strides(shape, perm):
+    """relayout_by_perm strides (array.rs:799-817)."""
+    pshape = [shape[a] for a in perm]
+    pst = c_strides(pshape)
+    st = [0] * len(shape)
+    for i, a in enumerate(perm):
+        st[a] = pst[i]
+    if int(np.prod(shape)) == 0:
+        st = [0] * len(shape)
+    return st
+
+
+def _is_contig(a: np.ndarray, f: bool):
+    return a.flags["F_CONTIGUOUS"] if f else a.flags["C_CONTIGUOUS"]
+
+
+def order_k_strides(out_shape, operands):
+    """Element strides of an order='K' ufunc result (lib.rs:1290-1330)."""
+    nd = len(out_shape)
+    if all(_is_contig(o, False) for o in operands):
+        perm = list(range(nd))
+    elif all(_is_contig(o, True) for o in operands):
+        perm = list(range(nd))[::-1]
+    else:
+        perm = multi_sorted_stride_perm(nd, [(o.shape, elem_strides(o)) for o in operands])
+    return perm_strides(list(out_shape), perm)
+
+
+def reduce_layout_strides(shape, strides, axes, keepdims):
+    """Strides of a reduction result (array.rs:845-930)."""
+    nd = len(shape)
+    retained = [i for i in range(nd) if i not in axes]
+    full = sorted(range(nd), key=lambda x: -abs(strides[x]))
+    local = {ax: i for i, ax in enumerate(retained)}
+    local_perm = [local[ax] for ax in full if ax in local]
+    kshape = [shape[a] for a in retained]
+    st = perm_strides(kshape, local_perm)
+    if not keepdims:
+        return st
+    pretend = list(shape)
+    for a in axes:
+        pretend[a] = 1
+    perm = sorted(range(nd), key=lambda x: -abs(strides[x]))
+    pshape = [pretend[a] for a in perm]
+    pst = c_strides(pshape)
+    full_st = [0] * nd
+    for i, a in enumerate(perm):
+        full_st[a] = pst[i]
+    if int(np.prod(pretend)) == 0:
+        full_st = [0] * nd
+    return full_st

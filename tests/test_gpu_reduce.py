@@ -1,0 +1,173 @@
+"""GPU parity of ufunc.reduce and argmin/argmax against the oracle:
+pairwise-exact float add (wide runs, narrow axes, multi-run layouts, split
+trees), f16 widening rules, sequential/associative folds, keepdims/initial/
+where/dtype/out=, output layout, and the reference's error cases."""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from tests._util import ALL, FLOATS, array, assert_bits_equal, values
+
+ap = pytest.importorskip("anionpy_b200")
+pytestmark = pytest.mark.gpu
+
+RED_OPS = ["add", "multiply", "maximum", "minimum", "subtract", "divide", "floor_divide", "logical_and",
+           "logical_or", "logical_xor", "bitwise_and", "bitwise_or", "bitwise_xor", "equal", "less"]
+
+
+def to_host(r):
+    return r.get() if isinstance(r, ap.ndarray) else np.asarray(r)
+
+
+def check_reduce(op, a_np, dev, axis=0, **kw):
+    try:
+        want = O.reduce(op, a_np, axis=axis, **kw)
+        werr = None
+    except O.OracleError as e:
+        want, werr = None, e.status
+    if werr is not None:
+        with pytest.raises((TypeError, ValueError)):
+            getattr(ap, op).reduce(dev, axis=axis, **kw)
+        return
+    dkw = dict(kw)
+    if "where" in dkw and isinstance(dkw["where"], np.ndarray):
+        dkw["where"] = ap.from_numpy(dkw["where"])
+    got = getattr(ap, op).reduce(dev, axis=axis, **dkw)
+    assert_bits_equal(to_host(got), np.asarray(want), f"{op}.reduce {a_np.dtype}{a_np.shape} axis={axis} {kw}")
+    if isinstance(got, ap.ndarray):
+        axes = O.normalize_reduce_axes(axis, a_np.ndim)
+        want_st = O.reduce_layout_strides(list(a_np.shape), O.elem_strides(a_np), axes, kw.get("keepdims", False))
+        assert list(got.elem_strides) == list(want_st), f"{op} strides {got.elem_strides} != {want_st}"
+
+
+@pytest.mark.parametrize("op", RED_OPS)
+@pytest.mark.parametrize("dt", ALL, ids=lambda d: np.dtype(d).name)
+def test_reduce_ops_dtypes(op, dt):
+    rng = np.random.default_rng(21)
+    a = array(dt, (37, 53), rng)
+    d = ap.from_numpy(a)
+    for axis in (0, 1, -1, None, (0, 1)):
+        check_reduce(op, a, d, axis=axis)
+
+
+PW_LENGTHS = [1, 2, 4, 7, 8, 9, 16, 31, 32, 64, 127, 128, 129, 136, 255, 256, 257, 1000, 1024, 4095, 4096, 5003,
+              65536, 65537, 100003, 262147]
+
+
+@pytest.mark.parametrize("dt", [np.float32, np.float64, np.float16], ids=lambda d: np.dtype(d).name)
+@pytest.mark.parametrize("n", PW_LENGTHS)
+def test_pairwise_lengths(dt, n):
+    rng = np.random.default_rng(n)
+    a = (rng.standard_normal(n) * 100).astype(dt)
+    check_reduce("add", a, ap.from_numpy(a), axis=0)
+    check_reduce("add", a, ap.from_numpy(a), axis=None, initial=2.5)
+
+
+@pytest.mark.parametrize("shape,axis", [((8, 32768), -1), ((64, 1000), 1), ((1024, 1024), 1), ((3, 5, 16), -1),
+                                        ((2, 3, 4, 5), (2, 3)), ((4, 5, 6), (0, 2)), ((6, 7, 8), None), ((16, 3, 5), 0),
+                                        ((5, 4096), None), ((1, 7), 0), ((7, 1), 1)])
+@pytest.mark.parametrize("dt", [np.float32, np.float64, np.float16], ids=lambda d: np.dtype(d).name)
+@pytest.mark.parametrize("layout", ["C", "F", "T", "step"])
+def test_float_add_layouts(shape, axis, dt, layout):
+    rng = np.random.default_rng(31)
+    base = array(dt, shape, rng)
+    if layout == "F":
+        a = np.asfortranarray(base)
+        d = ap.from_numpy(a)
+    elif layout == "T":
+        a = base.T
+        d = ap.from_numpy(base).T
+        axis = tuple(base.ndim - 1 - x for x in (axis if isinstance(axis, tuple) else (axis,))) if axis is not None else None
+        if isinstance(axis, tuple) and len(axis) == 1:
+            axis = axis[0]
+    elif layout == "step":
+        big = array(dt, shape[:-1] + (shape[-1] * 2,), rng)
+        a = big[..., ::2]
+        d = ap.from_numpy(big)[..., ::2]
+    else:
+        a, d = base, ap.from_numpy(base)
+    for kw in ({}, {"keepdims": True}, {"initial": 0.0, "keepdims": True}):
+        check_reduce("add", a, d, axis=axis, **kw)
+    check_reduce("multiply", a, d, axis=axis)
+    check_reduce("maximum", a, d, axis=axis)
+
+
+@pytest.mark.parametrize("dt", [np.float32, np.float64, np.float16, np.int32, np.int64, np.uint8, np.bool_],
+                         ids=lambda d: np.dtype(d).name)
+def test_where_initial_dtype(dt):
+    rng = np.random.default_rng(41)
+    a = array(dt, (23, 41), rng)
+    d = ap.from_numpy(a)
+    mask = rng.random((23, 41)) < 0.6
+    for axis in (0, 1, None):
+        check_reduce("add", a, d, axis=axis, where=mask)
+        check_reduce("maximum", a, d, axis=axis, where=mask, initial=-5)
+        check_reduce("add", a, d, axis=axis, initial=3)
+        check_reduce("add", a, d, axis=axis, dtype=np.float64)
+    check_reduce("add", a, d, axis=1, where=mask[0])  # broadcast mask
+    # a mask without identity or initial is an error
+    with pytest.raises(ValueError, match="identity"):
+        ap.maximum.reduce(d, axis=0, where=ap.from_numpy(mask))
+
+
+def test_empty_and_errors():
+    e = np.zeros((0, 5), np.float64)
+    de = ap.from_numpy(e)
+    assert_bits_equal(ap.add.reduce(de, axis=0).get(), O.reduce("add", e, axis=0), "empty add")
+    with pytest.raises(ValueError, match="zero-size array to reduction operation maximum"):
+        ap.maximum.reduce(de, axis=0)
+    with pytest.raises(ValueError, match="not reorderable"):
+        ap.subtract.reduce(ap.from_numpy(np.ones((2, 3))), axis=None)
+    with pytest.raises(TypeError):
+        ap.less.reduce(ap.from_numpy(np.ones(3)))
+    with pytest.raises(ap.AxisError):
+        ap.add.reduce(ap.from_numpy(np.ones(3)), axis=2)
+
+
+def test_out_param():
+    rng = np.random.default_rng(2)
+    a = array(np.float32, (40, 30), rng)
+    out = ap.empty((30,), np.float64)
+    r = ap.add.reduce(ap.from_numpy(a), axis=0, out=out)
+    assert r is out
+    assert_bits_equal(out.get(), O.reduce("add", a, axis=0).astype(np.float64), "out=")
+
+
+# ---------------------------------------------------------------- argext
+@pytest.mark.parametrize("which", ["argmax", "argmin"])
+@pytest.mark.parametrize("dt", ALL, ids=lambda d: np.dtype(d).name)
+def test_argext(which, dt):
+    rng = np.random.default_rng(51)
+    a = array(dt, (33, 70), rng)
+    if np.dtype(dt).kind in "iub":
+        a = (a % 5).astype(dt) if dt != np.bool_ else a  # many ties
+    d = ap.from_numpy(a)
+    for axis in (None, 0, 1, -1):
+        for kd in (False, True):
+            want = O.argext(which, a, axis=axis, keepdims=kd)
+            got = getattr(ap, which)(d, axis=axis, keepdims=kd)
+            assert_bits_equal(to_host(got), np.asarray(want), f"{which} axis={axis} keepdims={kd}")
+    # transposed and strided views
+    for v, dv in ((a.T, d.T), (a[:, ::3], d[:, ::3]), (a[::-1], d[::-1])):
+        for axis in (None, 0, 1):
+            assert_bits_equal(to_host(getattr(ap, which)(dv, axis=axis)), np.asarray(O.argext(which, v, axis=axis)),
+                              f"{which} view axis={axis}")
+
+
+@pytest.mark.parametrize("n", [1, 5, 64, 4097, 100000, 1 << 20])
+def test_argext_long(n):
+    rng = np.random.default_rng(n)
+    a = rng.standard_normal(n).astype(np.float32)
+    if n > 10:
+        a[n // 3] = np.nan
+        a[2 * n // 3] = np.nan
+    assert ap.argmax(ap.from_numpy(a)) == O.argext("argmax", a)
+    b = rng.integers(0, 3, (4, n)).astype(np.int64)
+    assert_bits_equal(ap.argmin(ap.from_numpy(b), axis=1).get(), O.argext("argmin", b, axis=1), "argmin rows")
+
+
+def test_argext_errors():
+    with pytest.raises(ValueError, match="empty sequence"):
+        ap.argmax(ap.from_numpy(np.zeros(0)))
+    with pytest.raises(ap.AxisError):
+        ap.argmin(ap.from_numpy(np.zeros((2, 2))), axis=2)
