@@ -74,6 +74,25 @@ def _operands(args):
     return out
 
 
+def _fmt_shape(s):
+    return "(" + ",".join(str(d) for d in s) + ("," if len(s) == 1 else "") + ")"
+
+
+def _broadcast(shapes):
+    """broadcast_shapes with the reference's error text (shape.rs:54-72)."""
+    nd = max((len(s) for s in shapes), default=0)
+    out = [1] * nd
+    for s in shapes:
+        for i, d in enumerate(s):
+            k = nd - len(s) + i
+            if out[k] == 1:
+                out[k] = d
+            elif d != 1 and d != out[k]:
+                raise ValueError("operands could not be broadcast together with shapes "
+                                 + " ".join(_fmt_shape(x) for x in shapes) + " ")
+    return tuple(out)
+
+
 def _scalar_result(r: ndarray):
     """A 0-d result becomes a numpy scalar (numpy_scalar_from_0d, lib.rs:8518)."""
     return r.get().reshape(())[()]
@@ -163,14 +182,14 @@ class ufunc:
             if loop is not None and any(o.dtype != loop for o in ops):
                 raise UFuncTypeError(f"Cannot cast ufunc '{self.__name__}' input from {ops[0].dtype!r} to {loop!r} with casting rule '{casting}'")
         rd = self._result_dtype([o.dtype for o in ops])
-        shape = np.broadcast_shapes(*[o.shape for o in ops]) if self.nin == 2 else ops[0].shape
+        shape = _broadcast([o.shape for o in ops]) if self.nin == 2 else ops[0].shape
         fpe = ctypes.c_uint32(0)
         want_fpe = self._fpe is not None
         if out is not None:
             if not isinstance(out, ndarray):
                 raise TypeError("return arrays must be of ArrayType")
-            np.broadcast_shapes(*[o.shape for o in orig], out.shape)
-            if tuple(np.broadcast_shapes(shape, out.shape)) != out.shape:
+            _broadcast([o.shape for o in orig] + [out.shape])
+            if tuple(_broadcast([shape, out.shape])) != out.shape:
                 raise ValueError(f"non-broadcastable output operand with shape {out.shape} doesn't match the broadcast shape {shape}")
             if not _can_cast(rd, out.dtype, rule):
                 raise UFuncTypeError(f"Cannot cast ufunc '{self.__name__}' output from {rd!r} to {out.dtype!r} with casting rule '{casting}'")

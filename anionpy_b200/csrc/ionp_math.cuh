@@ -18,8 +18,7 @@ template <int OP, int CD> struct UnOp {
             else if constexpr (dt_is_sint(CD)) return NEG ? w_sub<T>((T)0, x) : ABS ? (x < 0 ? w_sub<T>((T)0, x) : x) : (T)~x;
             else if constexpr (dt_is_uint(CD)) return NEG ? w_sub<T>((T)0, x) : ABS ? x : (T)~x;
             else if constexpr (CD == DT_F16) return NEG ? (T)(x ^ 0x8000u) : (T)(x & 0x7FFFu);
-            else if constexpr (CD == DT_F32) return bf(NEG ? (fb(x) ^ 0x80000000u) : (fb(x) & 0x7FFFFFFFu));
-            else return bd(NEG ? (db(x) ^ 0x8000000000000000ull) : (db(x) & 0x7FFFFFFFFFFFFFFFull));
+            else return NEG ? neg_bits(x) : abs_bits(x);
         } else {
             // math unary on float loop dtypes; float16 goes through f32
             if constexpr (CD == DT_F16) return f2h(f32op(h2f(x)));

@@ -102,6 +102,11 @@ template <int CD> __device__ __forceinline__ typename DT<CD>::T load_int_widen(c
 // Accumulation policy of the pairwise/tree kernels.
 template <int OP, int CD, bool CASTLD = false> struct RPol {
     static constexpr bool F16W = (CD == DT_F16 && OP == OP_ADD);
+    // float max/min pick the first NaN (and f16 the first of equal values) in
+    // fold order, so their leaves take contiguous chunks per lane; the float
+    // pairwise add needs the 8 interleaved accumulators; the integer, bool,
+    // bitwise and logical folds are order-free.
+    static constexpr bool CHUNK = dt_is_float(CD) && (OP == OP_MAXIMUM || OP == OP_MINIMUM);
     static constexpr int AD = F16W ? DT_F32 : CD;
     typedef typename DT<CD>::T T;
     typedef typename DT<AD>::T A;
@@ -164,6 +169,25 @@ __device__ __forceinline__ void seg_of(int64_t n, int K, int64_t path, int64_t* 
 template <class P>
 __device__ __forceinline__ typename P::A leaf_octet(const void* p, int sdt, int64_t base, int64_t ws, int64_t off, int64_t len, int j) {
     typedef typename P::A A;
+    if constexpr (P::CHUNK) {
+        // lane j folds [j*len/8, (j+1)*len/8) in order (len >= 8: no lane is empty)
+        const int64_t b0 = off + (j * len) / 8, b1 = off + ((j + 1) * len) / 8;
+        A r = P::load(p, base + b0 * ws, sdt);
+        A x[15];
+#pragma unroll
+        for (int i = 0; i < 15; ++i)
+            if (b0 + 1 + i < b1) x[i] = P::load(p, base + (b0 + 1 + i) * ws, sdt);
+#pragma unroll
+        for (int i = 0; i < 15; ++i)
+            if (b0 + 1 + i < b1) r = P::fold(r, x[i]);
+        const unsigned cmask = 0xFFu << ((threadIdx.x & 31) & ~7u);
+#pragma unroll
+        for (int s = 1; s < 8; s <<= 1) {
+            A other = __shfl_down_sync(cmask, r, s, 8);
+            if ((j & (2 * s - 1)) == 0) r = P::fold(r, other);
+        }
+        return r;
+    }
     const int64_t lim = len - len % 8;
     A r = P::load(p, base + (off + j) * ws, sdt);
     A x[15];

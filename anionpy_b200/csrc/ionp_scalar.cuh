@@ -46,6 +46,29 @@ __device__ __forceinline__ float bf(uint32_t u) { return __uint_as_float(u); }
 __device__ __forceinline__ uint64_t db(double d) { return (uint64_t)__double_as_longlong(d); }
 __device__ __forceinline__ double bd(uint64_t u) { return __longlong_as_double((long long)u); }
 
+// Sign-bit flips / clears done as integer ops in PTX: the compiler must not
+// turn them into floating-point negate/abs, which canonicalise NaN payloads.
+__device__ __forceinline__ float neg_bits(float x) {
+    uint32_t r;
+    asm("xor.b32 %0, %1, 0x80000000;" : "=r"(r) : "r"(__float_as_uint(x)));
+    return __uint_as_float(r);
+}
+__device__ __forceinline__ float abs_bits(float x) {
+    uint32_t r;
+    asm("and.b32 %0, %1, 0x7FFFFFFF;" : "=r"(r) : "r"(__float_as_uint(x)));
+    return __uint_as_float(r);
+}
+__device__ __forceinline__ double neg_bits(double x) {
+    uint64_t r;
+    asm("xor.b64 %0, %1, 0x8000000000000000;" : "=l"(r) : "l"((uint64_t)__double_as_longlong(x)));
+    return __longlong_as_double((long long)r);
+}
+__device__ __forceinline__ double abs_bits(double x) {
+    uint64_t r;
+    asm("and.b64 %0, %1, 0x7FFFFFFFFFFFFFFF;" : "=l"(r) : "l"((uint64_t)__double_as_longlong(x)));
+    return __longlong_as_double((long long)r);
+}
+
 __device__ __forceinline__ bool isnan_f(float x) { return (fb(x) & 0x7FFFFFFFu) > 0x7F800000u; }
 __device__ __forceinline__ bool isnan_d(double x) { return (db(x) & 0x7FFFFFFFFFFFFFFFull) > 0x7FF0000000000000ull; }
 __device__ __forceinline__ float quiet_f(float x) { return bf(fb(x) | 0x00400000u); }

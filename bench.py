@@ -277,6 +277,7 @@ def main():
     ap_.add_argument("--elements", type=int, default=N_ELEM, help="elements per operand (default 2^28)")
     ap_.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline leg")
     ap_.add_argument("--no-e2e", action="store_true")
+    ap_.add_argument("--only", default=None, help="run only the sweep cases whose name contains this")
     args = ap_.parse_args()
     if args.impl == "reference":
         return reference_arm(args)
@@ -302,6 +303,8 @@ def main():
     hbm_peak, peak_kind = peaks()
 
     cases, bufs = build_cases(ap, L, n)
+    if args.only:
+        cases = [c for c in cases if args.only in c[0]]
     outs = {}
     ev = [ctypes.c_void_p() for _ in range(len(cases) + 1)]
     for e in ev:
@@ -360,7 +363,7 @@ def main():
         gbs = (c[5] + c[6]) / (ms / 1e3) / 1e9
         rows.append({"case": c[0], "ms": round(float(ms), 4), "GB/s": round(gbs, 1), "frac": round(gbs / hbm_peak, 3)})
     dom = int(np.argmax(per_case))
-    head = [r for r in rows if r["case"] == "add/float32/contig"][0]
+    head = ([r for r in rows if r["case"] == "add/float32/contig"] or [rows[0]])[0]
 
     # parity on a sample of every case (full-size inputs, oracle on a stride)
     mismatches = 0

@@ -130,7 +130,10 @@ def binary(op: str, a: np.ndarray, b: np.ndarray):
     a = np.asarray(a)
     b = np.asarray(b)
     od = binary_out_dtype(op, a.dtype, b.dtype)
-    shape = np.broadcast_shapes(a.shape, b.shape)
+    try:
+        shape = np.broadcast_shapes(a.shape, b.shape)
+    except ValueError:
+        raise OracleError(1) from None
     out = np.empty(shape, od)
     fpe = ctypes.c_int(0)
     st = lib().oracle_binary(OPS[op], _desc(a), _desc(b), _desc(out), ctypes.byref(fpe))
