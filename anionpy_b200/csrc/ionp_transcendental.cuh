@@ -30,9 +30,9 @@ __device__ __forceinline__ bool round_pins(double y, float* out) {
     return __float_as_uint(a) == __float_as_uint(b);
 }
 
-__device__ __noinline__ float expf_slow(float x) { return dd::dd_to_float(dd::exp_dd((double)x)); }
-__device__ __noinline__ float logf_slow(float x) { return dd::dd_to_float(dd::log_dd((double)x)); }
-__device__ __noinline__ float sinf_slow(float x) { return dd::dd_to_float(dd::sin_dd((double)x)); }
+static __device__ __noinline__ float expf_slow(float x) { return dd::dd_to_float(dd::exp_dd((double)x)); }
+static __device__ __noinline__ float logf_slow(float x) { return dd::dd_to_float(dd::log_dd((double)x)); }
+static __device__ __noinline__ float sinf_slow(float x) { return dd::dd_to_float(dd::sin_dd((double)x)); }
 
 __device__ __forceinline__ float cr_expf(float x) {
     if (isnan_f(x)) return quiet_f(x);

@@ -66,7 +66,12 @@ def test_float32_correctly_rounded(fn):
     ref, _ = O.unary(fn, x)
     d = ulp_distance(got, ref)
     assert d.max() <= 1, f"{fn}: max ulp vs glibc {d.max()}"
-    assert np.count_nonzero(d) <= max(3, int(1e-3 * d.size)), f"{fn}: {np.count_nonzero(d)} differ from glibc"
+    # every disagreement with glibc is an argument where glibc itself is not
+    # correctly rounded (glibc 2.39 on x86-64: expf ~0.06%, logf ~0.01%,
+    # sinf ~1% of these inputs); wherever glibc is correctly rounded the
+    # results are identical bit for bit
+    glibc_cr = ulp_distance(ref, want) == 0
+    assert not np.any(d[glibc_cr & ~nan]), f"{fn}: differs from glibc where glibc is correctly rounded"
     assert got[nan].tobytes() == ref[nan].tobytes(), "NaN payloads"
 
 
