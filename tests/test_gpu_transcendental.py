@@ -6,9 +6,8 @@ ufunc_registry.py: exp 0, log 0, sin 1 for float32 / 0 for float64) are
 measured against NumPy on the reference's macOS host. On Linux the reference
 calls glibc, whose float32 expf/logf/sinf are not always correctly rounded
 (expf is off by up to ~0.5000001 ULP); these kernels are correctly rounded,
-so they agree with glibc wherever glibc is correctly rounded and differ by
-exactly 1 ULP elsewhere -- checked here as <= 1 ULP, with the disagreement
-rate bounded."""
+so they agree with glibc bit for bit wherever glibc is correctly rounded and
+differ by exactly 1 ULP elsewhere."""
 import mpmath
 import numpy as np
 import pytest
@@ -46,7 +45,8 @@ def cr_f64(fn, x):
     out = np.empty_like(x)
     f = {"exp": mpmath.exp, "log": mpmath.log, "sin": mpmath.sin}[fn]
     for i, v in enumerate(x):
-        if np.isnan(v) or np.isinf(v) or (fn == "log" and v <= 0) or (fn == "exp" and abs(v) > 800):
+        # zeros too: mpmath has no signed zero (sin(-0.0) is -0.0)
+        if np.isnan(v) or np.isinf(v) or v == 0 or (fn == "log" and v <= 0) or (fn == "exp" and abs(v) > 800):
             with np.errstate(all="ignore"):
                 out[i] = getattr(np, fn)(v)
             continue
