@@ -136,6 +136,34 @@ int32_t ionp_cast(const IonpArr* a, IonpArr* out, IonpStream stream);
 int32_t ionp_reduce(int32_t op, const IonpArr* a, const int32_t* axes, int32_t naxes, int32_t keepdims,
                     int32_t compute_dtype, const void* initial, const IonpArr* where, IonpArr* out,
                     IonpStream stream);
+/* ufunc.reduce that allocates no device memory. This entry point has no
+ * counterpart in the reference; it exists for callers that cannot let the
+ * library call cudaMalloc (a process that reserves its device memory up front
+ * and forbids later allocations, a host runtime that owns every device byte
+ * and passes in only its own buffers, a latency-critical loop that cannot
+ * afford an allocation's implicit synchronisation). It computes what
+ * ionp_reduce computes -- same arguments, minus the dtype override and the
+ * where= mask, with compute_dtype = reduce_family_compute_dtype -- but keeps
+ * the partial results of long runs in one fixed device array of
+ * IONP_NOALLOC_SCRATCH_BYTES inside the library, which every GPU that loads
+ * the library holds until the process exits. It never calls cudaMalloc,
+ * cudaFree or the library's caching allocator.
+ *   - Handles the layouts the row (pairwise-tree) kernels reduce in place:
+ *     the reduced axes form one run holding the smallest strides, input in
+ *     the compute dtype (integer add/multiply widening on load is allowed),
+ *     non-empty reduced extent. Others return IONP_ERR_UNSUPPORTED.
+ *   - Returns IONP_ERR_VALUE when the partials of a call would exceed
+ *     IONP_NOALLOC_SCRATCH_BYTES (at most 2^17 float64 partials: e.g. one
+ *     output up to 2^33 elements, or up to 2^17 outputs of runs longer than
+ *     65536 elements).
+ *   - The first call on a device looks up the array's device address with
+ *     that device current; make that first call before any stream capture.
+ *   - All calls share the one array: calls that overlap on the GPU (on
+ *     different streams, or from several threads) race on it. Serialise them
+ *     on one stream. */
+#define IONP_NOALLOC_SCRATCH_BYTES (1u << 20)
+int32_t ionp_reduce_noalloc(int32_t op, const IonpArr* a, const int32_t* axes, int32_t naxes, int32_t keepdims,
+                            const void* initial, IonpArr* out, IonpStream stream);
 /* argmin (is_max=0) / argmax (is_max=1): argext (ufunc.rs:8131) behind
  * do_argext (ionp-py/src/reductions.rs:1198). axis = -1 means the flattened
  * C-order ravel (axis=None); out is int64 with the kept shape. */
