@@ -1,15 +1,23 @@
 #!/usr/bin/env python
-"""Benchmark of the B200 ufunc engine on the large element-wise sweep.
+"""Benchmark of the B200 ufunc engine: the large element-wise sweep plus the
+reductions, in one step.
 
-Workload (one step = one pass over the whole sweep, 2^28 elements per
-operand): binary add, multiply, maximum, floor_divide, remainder and
-bitwise_and on int32/int64 (uniform over the full range, 1% zero divisors),
-the same arithmetic ufuncs on float32/float64 (N(0,1) with 0.1% NaN, 0.1%
-+-inf, 0.1% signed zeros), unary exp (U[-100,100]) / log (U(0,1e6]) / sin
-(10*N(0,1)) on float32/float64; every case contiguous, on a transposed
-(16384, 16384) view and on a step-2 slice of a 2^29 base. Inputs are seeded
-synthetic data resident in HBM (1-8 GiB per operand, far larger than the
-126 MB L2, so no flush is needed between steps).
+Element-wise part (2^28 elements per operand): binary add, multiply,
+maximum, floor_divide, remainder and bitwise_and on int32/int64 (uniform over
+the full range, 1% zero divisors), the same arithmetic ufuncs on
+float32/float64 (N(0,1) with 0.1% NaN, 0.1% +-inf, 0.1% signed zeros), unary
+exp (U[-100,100]) / log (U(0,1e6]) / sin (10*N(0,1)) on float32/float64;
+every case contiguous, on a transposed (16384, 16384) view and on a step-2
+slice of a 2^29 base.
+
+Reduction part: add.reduce, maximum.reduce and argmax over axis 0, -1 and
+all axes of float32 (8192, 32768) N(0,1) with 0.1% NaN, float64
+(4096, 4096, 16) N(0,1) with keepdims=True and initial=0.0, and int64 (2^27,)
+uniform in [-2^62, 2^62) (the sum wraps).
+
+Inputs are seeded synthetic data resident in HBM (1-8 GiB per operand, far
+larger than the 126 MB L2, so no flush is needed between steps). One step =
+one pass over every case; `value` = logical bytes of all cases / device time.
 
 Prints one JSON line (rank 0). --impl reference times the CPU restatement of
 the reference's engine on the host cores instead.
@@ -127,6 +135,111 @@ def build_cases(ap, L, n):
     return cases, bufs
 
 
+# ---------------------------------------------------------------------------
+# reductions: add.reduce / maximum.reduce / argmax over axis 0, -1 and all axes
+# ---------------------------------------------------------------------------
+RED_OPS = ["add", "maximum", "argmax"]
+RED_AXES = [0, -1, None]
+
+
+def reduce_inputs(scale=1):
+    """(name, host array, keepdims, initial) of the three reduction inputs:
+    float32 (8192, 32768) N(0,1) with 0.1% NaN; float64 (4096, 4096, 16)
+    N(0,1) reduced with keepdims=True and initial=0.0; int64 (2^27,) uniform
+    in [-2^62, 2^62) so the sum wraps. `scale` divides the leading extent
+    (small runs of the same shapes)."""
+    rng = np.random.default_rng(31)
+    f32 = rng.standard_normal((8192 // scale, 32768), dtype=np.float32)
+    f32.reshape(-1)[rng.random(f32.size) < 0.001] = np.nan
+    f64 = rng.standard_normal((4096 // scale, 4096, 16))
+    i64 = rng.integers(-(1 << 62), 1 << 62, (1 << 27) // scale, dtype=np.int64)
+    return [("float32(8192,32768)", f32, False, None), ("float64(4096,4096,16)", f64, True, 0.0),
+            ("int64(2^27,)", i64, False, None)]
+
+
+class ReduceCase:
+    """One reduction launched straight through the C ABI (ionp_reduce /
+    ionp_argext) into a preallocated device output, so the timed loop never
+    waits on the host."""
+
+    def __init__(self, ap, L, name, op, dev, host, axis, keepdims, initial):
+        from anionpy_b200 import _lib
+        self.name, self.op, self.dev, self.host = name, op, dev, host
+        self.axis, self.keepdims, self.initial = axis, keepdims, initial
+        nd = dev.ndim
+        isz = dev.itemsize
+        if op == "argmax":
+            if axis is None:
+                self.ax = -1
+                shape = (1,) * nd if keepdims else ()
+            else:
+                self.ax = axis % nd
+                shape = tuple((1 if i == self.ax else dev.shape[i]) for i in range(nd) if keepdims or i != self.ax)
+            self.out = ap.ndarray.empty(shape, np.int64)
+            self.in_bytes = dev.size * isz
+            self.out_bytes = self.out.size * 8
+        else:
+            axes = list(range(nd)) if axis is None else [axis % nd]
+            self.axes = (ctypes.c_int32 * len(axes))(*axes)
+            self.naxes = len(axes)
+            r = ctypes.c_int32()
+            _lib.check(L.ionp_reduce_compute_dtype(ap.BINARY_OPS[op], _lib.code_of(dev.dtype), ctypes.byref(r)))
+            cd = _lib.DTYPES[r.value]
+            ond = ctypes.c_int32()
+            osh = (ctypes.c_int64 * 32)()
+            ost = (ctypes.c_int64 * 32)()
+            _lib.check(L.ionp_reduce_layout(ctypes.byref(dev._desc()), self.axes, self.naxes, int(keepdims),
+                                            ctypes.byref(ond), osh, ost))
+            self.out = ap.ndarray.empty(tuple(osh[i] for i in range(ond.value)), cd,
+                                        [ost[i] for i in range(ond.value)])
+            self.init = None
+            if initial is not None:
+                self.init = np.array([initial], dtype=cd)
+            self.in_bytes = dev.size * isz
+            self.out_bytes = self.out.size * cd.itemsize
+        self.nbytes = self.in_bytes + self.out_bytes
+        self._a = dev._desc()
+        self._o = self.out._desc()
+        self.L = L
+
+    def launch(self):
+        from anionpy_b200 import _lib
+        if self.op == "argmax":
+            _lib.check(self.L.ionp_argext(1, ctypes.byref(self._a), self.ax, int(self.keepdims), ctypes.byref(self._o), None))
+        else:
+            from anionpy_b200 import BINARY_OPS
+            _lib.check(self.L.ionp_reduce(BINARY_OPS[self.op], ctypes.byref(self._a), self.axes, self.naxes,
+                                          int(self.keepdims), -1,
+                                          self.init.ctypes.data if self.init is not None else None,
+                                          None, ctypes.byref(self._o), None))
+
+    def check(self):
+        """Whole result against the oracle, bit for bit."""
+        from oracle import oracle as O
+        got = self.out.get()
+        if self.op == "argmax":
+            want = np.asarray(O.argext("argmax", self.host, axis=self.axis, keepdims=self.keepdims), np.int64)
+        else:
+            kw = {"keepdims": self.keepdims}
+            if self.initial is not None:
+                kw["initial"] = self.initial
+            want = np.asarray(O.reduce(self.op, self.host, axis=self.axis, **kw))
+        return got.reshape(-1).tobytes() == want.reshape(-1).tobytes()
+
+
+def build_reduce_cases(ap, L, scale=1):
+    cases, keep = [], []
+    for tag, host, keepdims, initial in reduce_inputs(scale):
+        dev = ap.from_numpy(host)
+        keep.append(dev)
+        for op in RED_OPS:
+            for axis in RED_AXES:
+                init = initial if op != "argmax" else None
+                name = f"{op}.reduce/{tag}/axis={axis}" if op != "argmax" else f"argmax/{tag}/axis={axis}"
+                cases.append(ReduceCase(ap, L, name, op, dev, host, axis, keepdims, init))
+    return cases, keep
+
+
 def sample(x, stride=4099):
     """Every stride-th element (C order) of a device array, copied to host."""
     flat = x if x.ndim == 1 else x.copy().reshape(-1)
@@ -143,6 +256,29 @@ def run_case(ap, case, outs):
         outs[key] = out
         return out
     return uf(*operands, out=out)
+
+
+class SweepItem:
+    """One element-wise case of the sweep, launched through the public ufunc
+    API with a reused out= array."""
+
+    def __init__(self, ap, case, outs):
+        self.ap, self.case, self.outs = ap, case, outs
+        self.name = case[0]
+        self.nbytes = case[5] + case[6]
+
+    def launch(self):
+        return run_case(self.ap, self.case, self.outs)
+
+    def check(self):
+        from oracle import oracle as O
+        name, op, dt, lay, operands, _, _ = self.case
+        if op in UN_OPS:
+            return None  # transcendentals: ULP-checked in tests/, not bitwise here
+        out = self.launch()
+        hosts = [sample(o) for o in operands]
+        want = O.binary(op, *hosts)[0]
+        return sample(out).tobytes() == want.tobytes()
 
 
 # ---------------------------------------------------------------------------
@@ -277,7 +413,10 @@ def main():
     ap_.add_argument("--elements", type=int, default=N_ELEM, help="elements per operand (default 2^28)")
     ap_.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline leg")
     ap_.add_argument("--no-e2e", action="store_true")
-    ap_.add_argument("--only", default=None, help="run only the sweep cases whose name contains this")
+    ap_.add_argument("--only", default=None, help="run only the cases whose name contains this")
+    ap_.add_argument("--no-reduce", action="store_true", help="skip the reduction cases")
+    ap_.add_argument("--reduce-scale", type=int, default=1, help="divide the reductions' leading extent (small runs)")
+    ap_.add_argument("--no-parity", action="store_true", help="skip the oracle checks after the timed region")
     args = ap_.parse_args()
     if args.impl == "reference":
         return reference_arm(args)
@@ -306,7 +445,14 @@ def main():
     if args.only:
         cases = [c for c in cases if args.only in c[0]]
     outs = {}
-    ev = [ctypes.c_void_p() for _ in range(len(cases) + 1)]
+    items = [SweepItem(ap, c, outs) for c in cases]
+    red_keep = None
+    if not args.no_reduce:
+        rcases, red_keep = build_reduce_cases(ap, L, args.reduce_scale)
+        if args.only:
+            rcases = [c for c in rcases if args.only in c.name]
+        items += rcases
+    ev = [ctypes.c_void_p() for _ in range(len(items) + 1)]
     for e in ev:
         _lib.check(L.ionp_event_create(ctypes.byref(e)))
     t_start, t_stop = ctypes.c_void_p(), ctypes.c_void_p()
@@ -319,8 +465,8 @@ def main():
 
     # warm-up
     for _ in range(max(args.warmup, 1)):
-        for c in cases:
-            run_case(ap, c, outs)
+        for it in items:
+            it.launch()
     L.ionp_device_synchronize()
 
     clocks = Clocks(local)
@@ -328,15 +474,15 @@ def main():
     barrier()
     L.ionp_device_synchronize()
     launches0 = _lib.launch_count()
-    per_case = np.zeros(len(cases))
+    per_case = np.zeros(len(items))
     L.ionp_event_record(t_start, None)
     for _ in range(args.steps):
         L.ionp_event_record(ev[0], None)
-        for i, c in enumerate(cases):
-            run_case(ap, c, outs)
+        for i, it in enumerate(items):
+            it.launch()
             L.ionp_event_record(ev[i + 1], None)
         L.ionp_device_synchronize()
-        for i in range(len(cases)):
+        for i in range(len(items)):
             ms = ctypes.c_float()
             L.ionp_event_elapsed_ms(ev[i], ev[i + 1], ctypes.byref(ms))
             per_case[i] += ms.value
@@ -353,33 +499,33 @@ def main():
         t = torch.tensor([total_ms], device=f"cuda:{local}")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         total_ms = float(t.item())
-    step_bytes = sum(c[5] + c[6] for c in cases)
+    step_bytes = sum(it.nbytes for it in items)
     value = step_bytes * args.steps * world / (total_ms / 1e3) / 1e9
 
     # per-case achieved bandwidth and the dominant kernel's roofline
     per_case /= args.steps
     rows = []
-    for c, ms in zip(cases, per_case):
-        gbs = (c[5] + c[6]) / (ms / 1e3) / 1e9
-        rows.append({"case": c[0], "ms": round(float(ms), 4), "GB/s": round(gbs, 1), "frac": round(gbs / hbm_peak, 3)})
+    for it, ms in zip(items, per_case):
+        gbs = it.nbytes / (ms / 1e3) / 1e9
+        rows.append({"case": it.name, "ms": round(float(ms), 4), "GB/s": round(gbs, 1), "frac": round(gbs / hbm_peak, 3)})
     dom = int(np.argmax(per_case))
     head = ([r for r in rows if r["case"] == "add/float32/contig"] or [rows[0]])[0]
+    sweep_ms = float(sum(per_case[i] for i, it in enumerate(items) if isinstance(it, SweepItem)))
+    red_ms = float(sum(per_case[i] for i, it in enumerate(items) if isinstance(it, ReduceCase)))
+    sweep_b = sum(it.nbytes for it in items if isinstance(it, SweepItem))
+    red_b = sum(it.nbytes for it in items if isinstance(it, ReduceCase))
 
-    # parity on a sample of every case (full-size inputs, oracle on a stride)
+    # parity: element-wise cases on a strided sample of the full-size
+    # outputs; reductions on their whole outputs
     mismatches = 0
     checked = 0
-    if rank == 0:
-        from oracle import oracle as O
-        for c in cases:
-            name, op, dt, lay, operands, _, _ = c
-            out = run_case(ap, c, outs)
-            if op in UN_OPS:
-                continue  # transcendentals: ULP-checked in tests/, not bitwise here
-            hosts = [sample(o) for o in operands]
-            want = O.binary(op, *hosts)[0]
-            got = sample(out)
-            mismatches += int(got.tobytes() != want.tobytes())
+    if rank == 0 and not args.no_parity:
+        for it in items:
+            ok = it.check()
+            if ok is None:
+                continue
             checked += 1
+            mismatches += int(not ok)
 
     # end-to-end through the public API with pinned host buffers
     e2e = None
@@ -399,10 +545,19 @@ def main():
             "metric": METRIC, "value": round(value, 2), "unit": "GB/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(total_ms / args.steps, 3), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "mixed(int32,int64,f32,f64)", "data": "synthetic",
-            "config": {"workload": "large element-wise sweep: 6 binary ufuncs x int32/int64, 5 x float32/float64, "
-                                   "exp/log/sin x float32/float64; contiguous, transposed (16384,16384) view, step-2 slice",
-                       "elements_per_operand": n, "cases": len(cases), "l2": "inputs 1-8 GiB per operand > 126 MB L2, no flush",
-                       "parallelism": f"replicas x{world}"},
+            "config": {"workload": "large element-wise sweep (2^28 elements per operand: 6 binary ufuncs x int32/int64, "
+                                   "5 x float32/float64, exp/log/sin x float32/float64; contiguous, transposed "
+                                   "(16384,16384) view, step-2 slice) + reductions (add.reduce, maximum.reduce, argmax "
+                                   "over axis 0/-1/None of float32 (8192,32768), float64 (4096,4096,16) keepdims "
+                                   "initial=0.0, int64 (2^27,))",
+                       "elements_per_operand": n, "cases": len(items), "reduce_scale": args.reduce_scale,
+                       "l2": "inputs 1-8 GiB per operand > 126 MB L2, no flush", "parallelism": f"replicas x{world}"},
+            "parts": {"elementwise": {"GB/s": round(sweep_b / (sweep_ms / 1e3) / 1e9, 1) if sweep_ms else None,
+                                      "frac": round(sweep_b / (sweep_ms / 1e3) / 1e9 / hbm_peak, 3) if sweep_ms else None,
+                                      "ms": round(sweep_ms, 3)},
+                      "reduce": {"GB/s": round(red_b / (red_ms / 1e3) / 1e9, 1) if red_ms else None,
+                                 "frac": round(red_b / (red_ms / 1e3) / 1e9 / hbm_peak, 3) if red_ms else None,
+                                 "ms": round(red_ms, 3)}},
             "roofline": {"bound": "hbm", "kernel": rows[dom]["case"], "achieved": rows[dom]["GB/s"], "peak": hbm_peak,
                          "unit": "GB/s", "frac": rows[dom]["frac"], "traffic": None, "peak_kind": peak_kind,
                          "headline_add_f32_contig": head},
@@ -410,7 +565,8 @@ def main():
             "e2e": e2e,
             "gpu_launches": int(launches),
             "clocks": clk,
-            "parity": {"cases_checked": checked, "cases_with_mismatch": mismatches, "sample_stride": 4099},
+            "parity": {"cases_checked": checked, "cases_with_mismatch": mismatches,
+                       "how": "element-wise: every 4099th output element vs the oracle; reductions: whole outputs"},
             "cases": rows,
         }
         print(json.dumps(line), flush=True)
