@@ -7,6 +7,7 @@ C ABI of ``libionp_cuda.so`` (include/ionp_cuda.h). Results are bit-exact with
 anionpy's CPU path; errors and ``errstate`` behave the same way.
 """
 from ._array import array, asarray, empty, from_numpy, ndarray, ones, zeros
+from ._batch import Batch
 from ._fpstate import errstate, geterr, geterrcall, seterr, seterrcall
 from ._lib import AxisError, UFuncTypeError, launch_count
 from ._ufunc import (BINARY_OPS, UNARY_OPS, absolute, add, argmax, argmin, bitwise_and, bitwise_not, bitwise_or,
@@ -18,5 +19,5 @@ from ._ufunc import abs  # noqa: A001
 __all__ = [
     "ndarray", "array", "asarray", "empty", "zeros", "ones", "from_numpy",
     "errstate", "seterr", "geterr", "seterrcall", "geterrcall", "AxisError", "UFuncTypeError",
-    "ufunc", "argmax", "argmin", "launch_count",
+    "ufunc", "argmax", "argmin", "launch_count", "Batch",
 ] + list(BINARY_OPS) + list(UNARY_OPS) + ["true_divide", "mod", "abs", "bitwise_not"]

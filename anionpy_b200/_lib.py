@@ -44,7 +44,15 @@ class AxisError(ValueError, IndexError):
     """numpy's AxisError (both a ValueError and an IndexError)."""
 
 
+class IonpSchedule(ctypes.Structure):
+    _fields_ = [("block_tile", ctypes.c_int32), ("vec_width", ctypes.c_int32),
+                ("elems_per_thread", ctypes.c_int32), ("red_split", ctypes.c_int32)]
+
+
+NUM_SCHEDULES = 48
+
 _P = ctypes.POINTER(IonpArr)
+_S = ctypes.POINTER(IonpSchedule)
 _SIGS = {
     "ionp_promote": [ctypes.c_int32, ctypes.c_int32, ctypes.POINTER(ctypes.c_int32)],
     "ionp_binary_out_dtype": [ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.POINTER(ctypes.c_int32)],
@@ -79,6 +87,22 @@ _SIGS = {
     "ionp_event_record": [ctypes.c_void_p, ctypes.c_void_p],
     "ionp_event_elapsed_ms": [ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(ctypes.c_float)],
     "ionp_set_device": [ctypes.c_int32],
+    "ionp_reduce_noalloc": [ctypes.c_int32, _P, ctypes.POINTER(ctypes.c_int32), ctypes.c_int32, ctypes.c_int32,
+                            ctypes.c_void_p, _P, ctypes.c_void_p],
+    "ionp_schedule_from_index": [ctypes.c_int32, _S],
+    "ionp_batch_create": [ctypes.POINTER(ctypes.c_void_p)],
+    "ionp_batch_destroy": [ctypes.c_void_p],
+    "ionp_batch_add_binary": [ctypes.c_void_p, ctypes.c_int32, _P, _P, _P, _S, ctypes.POINTER(ctypes.c_int32)],
+    "ionp_batch_add_reduce": [ctypes.c_void_p, ctypes.c_int32, _P, ctypes.c_int32, ctypes.c_int32, _P, _S,
+                              ctypes.POINTER(ctypes.c_int32)],
+    "ionp_batch_set_schedule": [ctypes.c_void_p, ctypes.c_int32, _S],
+    "ionp_batch_finalize": [ctypes.c_void_p, ctypes.c_void_p],
+    "ionp_batch_run": [ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p],
+    "ionp_batch_run_per_call": [ctypes.c_void_p, ctypes.c_void_p],
+    "ionp_batch_fpe": [ctypes.c_void_p, ctypes.POINTER(ctypes.c_uint32), ctypes.c_void_p],
+    "ionp_batch_info": [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int64)],
+    "ionp_batch_time_call": [ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32, _S, ctypes.c_int32,
+                             ctypes.POINTER(ctypes.c_float), ctypes.c_void_p],
     "ionp_device_info": [ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_int32), ctypes.c_char_p, ctypes.c_size_t],
 }
 

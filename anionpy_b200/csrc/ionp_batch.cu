@@ -1,0 +1,930 @@
+// Batched execution of many small ufunc calls: one persistent kernel drains a
+// device-side queue of call descriptors, captured once in a CUDA graph and
+// replayed. The reference runs every call on its own (ionp-py/src/lib.rs:9205
+// __call__, lib.rs:9959 reduce); this engine adds the batch so that a stream of
+// thousands of small calls costs one launch instead of thousands.
+//
+// Every call keeps the exact arithmetic of its standalone entry point: binary
+// calls use the same scalar op table (BinOp, cast on load to the loop dtype,
+// cast on store), reductions the same fold orders (pairwise tree on a
+// contiguous innermost run, sequential fold in row order otherwise, float16
+// widening, integer widening to int64/uint64). A call's schedule (block tile,
+// vector width, elements per thread, reduction split) only changes how its
+// work is cut into tiles and mapped to threads, never a result bit.
+//
+// Queue layout: call descriptors are stored in queue order (largest tiles
+// first, so the long reductions start early and the tail is short); a tile
+// -> call map gives each global tile index its descriptor. CTAs claim tiles
+// with one atomicAdd on a global counter and copy the descriptor of a new
+// call into shared memory once. Reductions split in two (schedule
+// red_split = 2) combine their halves with a last-arriver counter: the CTA
+// that finishes second folds (left, right) in order, so no CTA ever waits.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <numeric>
+#include <vector>
+#include "ionp_host.h"
+#include "ionp_reduce_launch.cuh"
+#include "ionp_ew_launch.cuh"
+
+namespace ionp {
+namespace {
+
+constexpr int BT_THREADS = 256;
+enum : int32_t { BK_BINARY = 0, BK_ROW = 1, BK_COL = 2 };
+
+// n / d for 0 <= n < 2^31, 1 <= d < 2^31, as one multiply and shift:
+// m = ceil(2^(32+s) / d) with 2^s >= d makes the error term smaller than the
+// distance from n/d to the next integer.
+struct FastDiv {
+    uint64_t m;
+    uint32_t d;
+    int32_t s;
+};
+FastDiv make_div(uint32_t d) {
+    FastDiv f;
+    f.d = d ? d : 1;
+    f.s = 0;
+    while ((1ull << f.s) < f.d) ++f.s;
+    f.m = ((1ull << (32 + f.s)) + f.d - 1) / f.d;
+    return f;
+}
+__device__ __forceinline__ uint32_t fdiv(uint32_t n, const FastDiv& f) {
+    return (uint32_t)(((uint64_t)n * f.m) >> (32 + f.s));
+}
+
+// Device descriptor of one call (queue entry).
+struct BatchCall {
+    int32_t kind, op, cd;
+    int32_t dta, dtb, dto;
+    int32_t nd;          // binary: merged dims (1..4)
+    int32_t vec;         // binary: 16-byte vector path
+    int32_t a_sc, b_sc;  // vector path: 0-d operand
+    int32_t tpr, D;      // row: threads per output, slot-tree depth
+    int32_t split;       // reduce: 1 or 2 tiles per output group
+    int32_t has_seed;
+    int32_t bt, vw, ept; // schedule
+    int32_t user_id;
+    int32_t shape[4];
+    FastDiv div[4];
+    int64_t sa[4], sb[4], so[4];
+    const void* a;
+    const void* b;
+    void* o;
+    int64_t n;           // binary: output elements; reduce: outputs
+    int64_t per_tile;    // binary: elements per tile; reduce: outputs per tile
+    int64_t ntiles;
+    int64_t tile0;
+    int64_t w, rs;       // reduce: extent and stride of the reduced axis
+    int64_t ostride;     // reduce: input distance between consecutive outer indices
+    int64_t inner;       // col: kept inner extent
+    FastDiv idiv;        // col: division by inner
+    uint64_t seed;
+    void* partial;       // split: two partials per output
+    uint32_t* arrive;    // split: arrival counter per output
+    uint32_t* flags;     // FPE word of the call
+};
+static_assert(sizeof(BatchCall) % 4 == 0, "descriptor copies as 32-bit words");
+
+// ------------------------------------------------------------------ binary
+// Tile bodies are separate (not inlined) device functions: the persistent
+// kernel dispatches over ~130 of them, and inlining them all into one body
+// makes register allocation of that body intractable.
+template <int OP, int CD>
+__device__ __noinline__ void bin_tile(const BatchCall& c, int64_t local) {
+    typedef BinOp<OP, CD> Op;
+    typedef typename DT<CD>::T T;
+    typedef typename Op::R R;
+    constexpr bool FPE = FpeKind<OP, CD>::value != 0;
+    // independent vectors / elements in flight per thread; float16 loops
+    // (software half arithmetic) keep one to bound the code size
+    constexpr int U = CD == DT_F16 ? 1 : 2;
+    uint32_t bits = 0;
+    const int nthr = c.bt < BT_THREADS ? c.bt : BT_THREADS;
+    const int tid = threadIdx.x;
+    const int64_t e0 = local * c.per_tile;
+    const int64_t e1 = (e0 + c.per_tile < c.n) ? e0 + c.per_tile : c.n;
+    R* o = (R*)c.o;  // the batch stores the loop's result dtype
+    if (c.vec) {
+        constexpr int N = Vec16<T>::N;
+        const T* a = (const T*)c.a;
+        const T* b = (const T*)c.b;
+        const T a0 = a[0], b0 = b[0];
+        const int64_t v0 = e0 / N, nv = e1 / N - v0;     // whole vectors of this tile
+        const int unit = c.vw;                              // consecutive vectors per unit
+        const int64_t per_pass = (int64_t)nthr * c.ept * unit;
+        if (tid < nthr) {
+            const int nmine = c.ept * unit;
+            for (int64_t p0 = 0; p0 < nv; p0 += per_pass) {
+                for (int q0 = 0; q0 < nmine; q0 += U) {
+                    Vec16<T> xa[U], xb[U];
+                    int64_t vi[U];
+#pragma unroll
+                    for (int j = 0; j < U; ++j) {
+                        const int q = q0 + j;
+                        const int k = q / unit, u = q - k * unit;
+                        vi[j] = p0 + ((int64_t)k * nthr + tid) * unit + u;
+                        if (q < nmine && vi[j] < nv) {
+                            if (!c.a_sc) xa[j] = ldv(a, v0 + vi[j]); else for (int i = 0; i < N; ++i) xa[j].v[i] = a0;
+                            if (!c.b_sc) xb[j] = ldv(b, v0 + vi[j]); else for (int i = 0; i < N; ++i) xb[j].v[i] = b0;
+                        }
+                    }
+#pragma unroll
+                    for (int j = 0; j < U; ++j) {
+                        if (q0 + j < nmine && vi[j] < nv) {
+                            R r[N];
+#pragma unroll
+                            for (int i = 0; i < N; ++i) {
+                                r[i] = Op::apply(xa[j].v[i], xb[j].v[i]);
+                                if constexpr (FPE) bits |= fpe_bits<OP, CD>(xa[j].v[i], xb[j].v[i], r[i]);
+                            }
+                            stv<R, N>(o, v0 + vi[j], r);
+                        }
+                    }
+                }
+            }
+            // ragged end of the call (only the last tile has one)
+            for (int64_t e = (v0 + nv) * N + tid; e < e1; e += nthr) {
+                T x = c.a_sc ? a0 : a[e], y = c.b_sc ? b0 : b[e];
+                R r = Op::apply(x, y);
+                if constexpr (FPE) bits |= fpe_bits<OP, CD>(x, y, r);
+                o[e] = r;
+            }
+        }
+    } else if (tid < nthr) {
+        const int nd = c.nd;
+        for (int64_t base = e0 + tid; base < e1; base += U * (int64_t)nthr) {
+            T x[U], y[U];
+            int64_t oo[U];
+#pragma unroll
+            for (int j = 0; j < U; ++j) {
+                const int64_t e = base + (int64_t)j * nthr;
+                if (e < e1) {
+                    uint32_t idx = (uint32_t)e;
+                    int64_t fa = 0, fb_ = 0, fo = 0;
+                    for (int k = nd - 1; k >= 1; --k) {
+                        uint32_t q = fdiv(idx, c.div[k]);
+                        uint32_t r = idx - q * (uint32_t)c.shape[k];
+                        fa += (int64_t)r * c.sa[k];
+                        fb_ += (int64_t)r * c.sb[k];
+                        fo += (int64_t)r * c.so[k];
+                        idx = q;
+                    }
+                    fa += (int64_t)idx * c.sa[0];
+                    fb_ += (int64_t)idx * c.sb[0];
+                    fo += (int64_t)idx * c.so[0];
+                    x[j] = load_cast<CD>(c.a, fa, c.dta);
+                    y[j] = load_cast<CD>(c.b, fb_, c.dtb);
+                    oo[j] = fo;
+                }
+            }
+#pragma unroll
+            for (int j = 0; j < U; ++j) {
+                if (base + (int64_t)j * nthr < e1) {
+                    R r = Op::apply(x[j], y[j]);
+                    if constexpr (FPE) bits |= fpe_bits<OP, CD>(x[j], y[j], r);
+                    o[oo[j]] = r;
+                }
+            }
+        }
+    }
+    if constexpr (FPE) flush_flags(bits, c.flags);
+}
+
+template <int OP>
+__device__ __forceinline__ void bin_dispatch(const BatchCall& c, int64_t local) {
+#define IONP_BCASE(D) \
+    case D:           \
+        if constexpr (bin_valid<OP, D>()) bin_tile<OP, D>(c, local); \
+        break;
+    switch (c.cd) { IONP_DTS(IONP_BCASE) }
+#undef IONP_BCASE
+}
+
+// --------------------------------------------------------------- reduction
+// Split combine: the tile that arrives second folds (left, right) in order.
+template <class P, int CD>
+__device__ __forceinline__ void split_combine(const BatchCall& c, int64_t o, int h, typename P::A part, bool is_final_value) {
+    typedef typename P::A A;
+    A* pp = reinterpret_cast<A*>(c.partial);
+    pp[2 * o + h] = part;
+    __threadfence();
+    const unsigned prev = atomicAdd(&c.arrive[o], 1u);
+    if (prev == 1u) {
+        __threadfence();
+        const A left = *(volatile A*)&pp[2 * o], right = *(volatile A*)&pp[2 * o + 1];
+        const A tot = P::fold(left, right);
+        if (is_final_value) store_cast<CD>(c.o, o, c.dto, (typename P::T)tot);
+        else store_cast<CD>(c.o, o, c.dto, P::finish(tot, c.has_seed, c.seed));
+    }
+}
+
+template <int OP, int CD, bool CASTLD, int TPR>
+__device__ __noinline__ void row_tile(const BatchCall& c, int64_t local, unsigned char* smem) {
+    typedef RPol<OP, CD, CASTLD> P;
+    typedef typename P::A A;
+    constexpr int G = BT_THREADS / TPR;
+    const int g = threadIdx.x / TPR, t = threadIdx.x % TPR;
+    const int nslots = TPR >= 32 ? (1 << c.D) : 1;
+    A* slots = reinterpret_cast<A*>(smem) + (size_t)g * nslots;
+    uint8_t* valid = reinterpret_cast<uint8_t*>(reinterpret_cast<A*>(smem) + (size_t)G * nslots) + (size_t)g * nslots;
+    if (c.split == 2) {
+        // TPR == 256: this tile is one half of one output's run, split at the
+        // root of the pairwise tree (any split for the associative ops)
+        if constexpr (TPR == BT_THREADS) {
+            const int64_t o = local >> 1;
+            const int h = (int)(local & 1);
+            const int64_t n2 = pw_split(c.w);
+            const int64_t soff = h ? n2 : 0, slen = h ? c.w - n2 : n2;
+            A r = group_tree_t<P, TPR>(c.a, c.dta, c.rs, o * c.ostride, soff, slen, c.D, slots, valid, t);
+            if (t == 0) split_combine<P, CD>(c, o, h, r, false);
+        }
+        return;
+    }
+    const int64_t o_first = local * c.per_tile;
+    for (int64_t k0 = 0; k0 < c.per_tile; k0 += G) {
+        const int64_t o = o_first + k0 + g;
+        const bool live = (k0 + g < c.per_tile) && o < c.n;
+        A r{};
+        if constexpr (TPR == 1) {
+            if (live) r = leaf_thread<P>(c.a, c.dta, o * c.ostride, c.rs, 0, c.w);
+        } else if constexpr (TPR == BT_THREADS) {
+            const int64_t oo = o_first + k0;
+            if (oo >= c.n) break;  // uniform over the CTA
+            r = group_tree_t<P, TPR>(c.a, c.dta, c.rs, oo * c.ostride, 0, c.w, c.D, slots, valid, t);
+        } else {
+            if (live) r = group_tree_t<P, TPR>(c.a, c.dta, c.rs, o * c.ostride, 0, c.w, c.D, slots, valid, t);
+        }
+        if (live && t == 0) store_cast<CD>(c.o, o, c.dto, P::finish(r, c.has_seed, c.seed));
+        if constexpr (TPR == BT_THREADS) __syncthreads();
+    }
+}
+
+template <int OP, int CD, bool CASTLD>
+__device__ __noinline__ void col_tile(const BatchCall& c, int64_t local) {
+    typedef typename DT<CD>::T T;
+    const int split = c.split;
+    const int64_t chunk = split == 2 ? local >> 1 : local;
+    const int h = split == 2 ? (int)(local & 1) : 0;
+    const int64_t half = c.w / 2;
+    const int64_t j0 = split == 2 && h ? half : 0;
+    const int64_t j1 = split == 2 && !h ? half : c.w;
+    const int64_t o0 = chunk * c.per_tile;
+    // raw compute-dtype loads (integer widening on load): the sequential
+    // folds run in the compute dtype itself, float16 included
+    auto ld = [&](int64_t e) -> T {
+        if constexpr (CASTLD) return load_int_widen<CD>(c.a, e, c.dta);
+        else return reinterpret_cast<const T*>(c.a)[e];
+    };
+    for (int64_t k = threadIdx.x; k < c.per_tile; k += BT_THREADS) {
+        const int64_t o = o0 + k;
+        if (o >= c.n) break;
+        const uint32_t outer = fdiv((uint32_t)o, c.idiv);
+        const int64_t in_ = o - (int64_t)outer * c.inner;
+        const int64_t base = (int64_t)outer * c.ostride + in_;
+        T acc;
+        bool have = false;
+        if (h == 0 && c.has_seed) { memcpy(&acc, &c.seed, sizeof(T)); have = true; }
+        int64_t j = j0;
+        for (; j + 8 <= j1; j += 8) {
+            T x[8];
+#pragma unroll
+            for (int u = 0; u < 8; ++u) x[u] = ld(base + (j + u) * c.rs);
+#pragma unroll
+            for (int u = 0; u < 8; ++u) {
+                if (!have) { acc = x[u]; have = true; }
+                else acc = BinOp<OP, CD>::apply(acc, x[u]);
+            }
+        }
+        for (; j < j1; ++j) {
+            T x = ld(base + j * c.rs);
+            if (!have) { acc = x; have = true; }
+            else acc = BinOp<OP, CD>::apply(acc, x);
+        }
+        if (split == 2) {
+            typedef RPol<OP, CD> PF;  // accumulator = compute dtype for the sequential folds
+            if constexpr (std::is_same<typename PF::A, T>::value) split_combine<PF, CD>(c, o, h, acc, true);
+        } else {
+            store_cast<CD>(c.o, o, c.dto, acc);
+        }
+    }
+}
+
+template <int OP, int CD, bool CASTLD>
+__device__ __forceinline__ void red_tile(const BatchCall& c, int64_t local, unsigned char* smem) {
+    if (c.kind == BK_COL) { col_tile<OP, CD, CASTLD>(c, local); return; }
+    switch (c.tpr) {
+        case 1: row_tile<OP, CD, CASTLD, 1>(c, local, smem); break;
+        case 32: row_tile<OP, CD, CASTLD, 32>(c, local, smem); break;
+        default: row_tile<OP, CD, CASTLD, BT_THREADS>(c, local, smem); break;
+    }
+}
+
+__device__ __forceinline__ void red_dispatch(const BatchCall& c, int64_t local, unsigned char* smem) {
+    if (c.op == OP_ADD) {
+        switch (c.cd) {
+            case DT_I64: red_tile<OP_ADD, DT_I64, true>(c, local, smem); break;
+            case DT_U64: red_tile<OP_ADD, DT_U64, true>(c, local, smem); break;
+            case DT_F16: red_tile<OP_ADD, DT_F16, false>(c, local, smem); break;
+            case DT_F32: red_tile<OP_ADD, DT_F32, false>(c, local, smem); break;
+            case DT_F64: red_tile<OP_ADD, DT_F64, false>(c, local, smem); break;
+        }
+        return;
+    }
+#define IONP_MCASE(D) \
+    case D: red_tile<OP_MAXIMUM, D, false>(c, local, smem); break;
+    switch (c.cd) { IONP_DTS(IONP_MCASE) }
+#undef IONP_MCASE
+}
+
+// The persistent kernel: claim tiles until the queue is drained.
+__global__ void __launch_bounds__(BT_THREADS) k_batch(const BatchCall* __restrict__ calls,
+                                                      const int32_t* __restrict__ tile_call, int64_t ntiles,
+                                                      unsigned long long* next) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    __shared__ BatchCall sc;
+    __shared__ int64_t s_tile;
+    __shared__ int32_t s_call;
+    int cur = -1;
+    for (;;) {
+        if (threadIdx.x == 0) {
+            const int64_t t = (int64_t)atomicAdd(next, 1ull);
+            s_tile = t;
+            s_call = t < ntiles ? tile_call[t] : -1;
+        }
+        __syncthreads();
+        const int64_t t = s_tile;
+        const int ci = s_call;
+        if (t >= ntiles) break;
+        if (ci != cur) {
+            const uint32_t* src = reinterpret_cast<const uint32_t*>(calls + ci);
+            uint32_t* dst = reinterpret_cast<uint32_t*>(&sc);
+            for (int i = threadIdx.x; i < (int)(sizeof(BatchCall) / 4); i += BT_THREADS) dst[i] = src[i];
+            cur = ci;
+            __syncthreads();
+        }
+        const int64_t local = t - sc.tile0;
+        if (sc.kind == BK_BINARY) {
+            switch (sc.op) {
+                case OP_ADD: bin_dispatch<OP_ADD>(sc, local); break;
+                case OP_SUBTRACT: bin_dispatch<OP_SUBTRACT>(sc, local); break;
+                case OP_MULTIPLY: bin_dispatch<OP_MULTIPLY>(sc, local); break;
+                case OP_MAXIMUM: bin_dispatch<OP_MAXIMUM>(sc, local); break;
+                case OP_LESS: bin_dispatch<OP_LESS>(sc, local); break;
+                case OP_LOGICAL_AND: bin_dispatch<OP_LOGICAL_AND>(sc, local); break;
+            }
+        } else {
+            red_dispatch(sc, local, smem);
+        }
+        __syncthreads();
+    }
+}
+
+int64_t ceil_div(int64_t a, int64_t b) { return (a + b - 1) / b; }
+
+int tree_depth(int64_t n) {
+    if (n <= PW_BLOCK) return 0;
+    int64_t n2 = pw_split(n);
+    return 1 + std::max(tree_depth(n2), tree_depth(n - n2));
+}
+
+bool c_contiguous(const IonpArr* a) {
+    int64_t acc = 1;
+    for (int i = a->ndim - 1; i >= 0; --i) {
+        if (a->shape[i] != 1 && a->strides[i] != acc) return false;
+        acc *= a->shape[i];
+    }
+    return true;
+}
+
+}  // namespace
+}  // namespace ionp
+
+using namespace ionp;
+
+// ===========================================================================
+// host side
+// ===========================================================================
+struct IonpBatch {
+    struct Orig {
+        int kind, op, axis, keepdims;
+        IonpArr a, b, out;
+    };
+    std::vector<BatchCall> calls;   // caller order
+    std::vector<Orig> orig;
+    std::vector<IonpSchedule> sched;
+    int device = 0;
+    int sms = 148;
+    // device state (from the caching allocator)
+    BatchCall* d_calls = nullptr;
+    int32_t* d_tile_call = nullptr;
+    unsigned long long* d_next = nullptr;
+    uint32_t* d_flags = nullptr;
+    void* d_partial = nullptr;
+    uint32_t* d_arrive = nullptr;
+    size_t partial_bytes = 0, arrive_bytes = 0;
+    int64_t ntiles = 0;
+    size_t smem = 0;
+    int grid = 0;
+    bool finalized = false;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t gexec = nullptr;
+    cudaStream_t capture_stream = nullptr;
+    // single-call timing area
+    BatchCall* d_one = nullptr;
+    int32_t* d_one_map = nullptr;
+    int64_t one_cap = 0;
+};
+
+namespace {
+
+void release_device(IonpBatch* b) {
+    cudaStream_t s = nullptr;
+    if (b->gexec) { cudaGraphExecDestroy(b->gexec); b->gexec = nullptr; }
+    if (b->graph) { cudaGraphDestroy(b->graph); b->graph = nullptr; }
+    if (b->d_calls) scratch_free(b->d_calls, s);
+    if (b->d_tile_call) scratch_free(b->d_tile_call, s);
+    if (b->d_next) scratch_free(b->d_next, s);
+    if (b->d_flags) scratch_free(b->d_flags, s);
+    if (b->d_partial) scratch_free(b->d_partial, s);
+    if (b->d_arrive) scratch_free(b->d_arrive, s);
+    if (b->d_one) scratch_free(b->d_one, s);
+    if (b->d_one_map) scratch_free(b->d_one_map, s);
+    b->d_calls = nullptr; b->d_tile_call = nullptr; b->d_next = nullptr; b->d_flags = nullptr;
+    b->d_partial = nullptr; b->d_arrive = nullptr; b->d_one = nullptr; b->d_one_map = nullptr;
+    b->one_cap = 0;
+    b->finalized = false;
+}
+
+int32_t check_schedule(const IonpSchedule* s) {
+    if (!s) return IONP_OK;
+    bool ok = (s->block_tile == 128 || s->block_tile == 256 || s->block_tile == 512 || s->block_tile == 1024) &&
+              (s->vec_width == 1 || s->vec_width == 2 || s->vec_width == 4) &&
+              (s->elems_per_thread == 1 || s->elems_per_thread == 4) && (s->red_split == 1 || s->red_split == 2);
+    return ok ? IONP_OK : set_err(IONP_ERR_INVALID, "schedule outside the 48-point space");
+}
+
+// Tile geometry of one call under its schedule (fills per_tile, ntiles,
+// split and D; everything else was planned when the call was added).
+void tile_call(BatchCall& c, const IonpSchedule& s) {
+    c.bt = s.block_tile;
+    c.vw = s.vec_width;
+    c.ept = s.elems_per_thread;
+    const int64_t work = (int64_t)s.block_tile * s.elems_per_thread * s.vec_width;
+    if (c.kind == BK_BINARY) {
+        const int64_t per = c.vec ? work * (16 / dt_size(c.cd)) : work * 4;
+        c.per_tile = per;
+        c.ntiles = ceil_div(c.n, per);
+        c.split = 1;
+        return;
+    }
+    const bool assoc = red_assoc(c.op, c.cd);
+    if (c.kind == BK_ROW) {
+        c.tpr = c.w <= PW_BLOCK ? 1 : c.w <= 2048 ? 32 : BT_THREADS;
+        c.split = (s.red_split == 2 && c.tpr == BT_THREADS) ? 2 : 1;
+        if (c.split == 2) {
+            const int64_t n2 = pw_split(c.w);
+            c.D = std::max(tree_depth(n2), tree_depth(c.w - n2));
+            c.per_tile = 1;
+            c.ntiles = 2 * c.n;
+        } else {
+            c.D = c.tpr >= 32 ? tree_depth(c.w) : 0;
+            c.per_tile = std::max<int64_t>(1, (work * 4) / std::max<int64_t>(c.w, 1));
+            if (c.tpr == 1) c.per_tile = std::max<int64_t>(c.per_tile, 1);
+            c.ntiles = ceil_div(c.n, c.per_tile);
+        }
+        return;
+    }
+    // column: the split halves the reduced extent, exact only for the
+    // associative folds
+    c.split = (s.red_split == 2 && assoc && c.w >= 2) ? 2 : 1;
+    c.per_tile = (int64_t)s.block_tile * s.elems_per_thread;
+    c.ntiles = ceil_div(c.n, c.per_tile) * c.split;
+}
+
+size_t row_smem(const BatchCall& c) {
+    if (c.kind != BK_ROW || c.tpr < 32) return 0;
+    size_t acc = (c.cd == DT_F16 && c.op == OP_ADD) ? 4 : (size_t)dt_size(c.cd);
+    size_t groups = BT_THREADS / c.tpr;
+    return groups * ((size_t)1 << c.D) * (acc + 1) + 16;
+}
+
+int64_t tile_cost(const BatchCall& c) {
+    if (c.kind == BK_BINARY) return c.per_tile * (dt_size(c.dta) + dt_size(c.dtb) + dt_size(c.dto));
+    if (c.kind == BK_ROW) return (c.split == 2 ? c.w / 2 : c.per_tile * c.w) * dt_size(c.dta);
+    return c.per_tile * (c.split == 2 ? c.w / 2 : c.w) * dt_size(c.dta);
+}
+
+void set_default_schedule(IonpSchedule* s) {
+    s->block_tile = 256;
+    s->vec_width = 1;
+    s->elems_per_thread = 4;
+    s->red_split = 1;
+}
+
+int32_t upload_and_plan(IonpBatch* b, cudaStream_t s) {
+    release_device(b);
+    const int nc = (int)b->calls.size();
+    std::vector<BatchCall> q(b->calls);
+    size_t smem = 0;
+    for (int i = 0; i < nc; ++i) {
+        tile_call(q[i], b->sched[i]);
+        smem = std::max(smem, row_smem(q[i]));
+    }
+    std::vector<int> order(nc);
+    std::iota(order.begin(), order.end(), 0);
+    std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return tile_cost(q[x]) > tile_cost(q[y]); });
+    std::vector<BatchCall> qq(nc);
+    int64_t tiles = 0;
+    size_t part = 0, arr = 0;
+    for (int k = 0; k < nc; ++k) {
+        qq[k] = q[order[k]];
+        qq[k].tile0 = tiles;
+        tiles += qq[k].ntiles;
+        if (qq[k].kind != BK_BINARY && qq[k].split == 2) {
+            part += (size_t)qq[k].n * 16;
+            arr += (size_t)qq[k].n * 4;
+        }
+    }
+    if (tiles >= (int64_t)1 << 31) return set_err(IONP_ERR_UNSUPPORTED, "batch has too many tiles");
+    std::vector<int32_t> map((size_t)tiles);
+    for (int k = 0; k < nc; ++k)
+        for (int64_t t = 0; t < qq[k].ntiles; ++t) map[(size_t)(qq[k].tile0 + t)] = k;
+    b->d_calls = (BatchCall*)scratch_alloc(sizeof(BatchCall) * std::max(nc, 1), s);
+    b->d_tile_call = (int32_t*)scratch_alloc(sizeof(int32_t) * std::max<int64_t>(tiles, 1), s);
+    b->d_next = (unsigned long long*)scratch_alloc(256, s);
+    b->d_flags = (uint32_t*)scratch_alloc(sizeof(uint32_t) * std::max(nc, 1), s);
+    if (part) {
+        b->d_partial = scratch_alloc(part, s);
+        b->d_arrive = (uint32_t*)scratch_alloc(arr, s);
+    }
+    if (!b->d_calls || !b->d_tile_call || !b->d_next || !b->d_flags || (part && (!b->d_partial || !b->d_arrive))) {
+        release_device(b);
+        return IONP_ERR_OOM;
+    }
+    b->partial_bytes = part;
+    b->arrive_bytes = arr;
+    size_t po = 0, ao = 0;
+    for (int k = 0; k < nc; ++k) {
+        BatchCall& c = qq[k];
+        c.flags = b->d_flags + c.user_id;
+        if (c.kind != BK_BINARY && c.split == 2) {
+            c.partial = (char*)b->d_partial + po;
+            c.arrive = (uint32_t*)((char*)b->d_arrive + ao);
+            po += (size_t)c.n * 16;
+            ao += (size_t)c.n * 4;
+        }
+    }
+    int32_t st;
+    if ((st = cuda_err(cudaMemcpyAsync(b->d_calls, qq.data(), sizeof(BatchCall) * nc, cudaMemcpyHostToDevice, s), "batch upload")))
+        return st;
+    if ((st = cuda_err(cudaMemcpyAsync(b->d_tile_call, map.data(), sizeof(int32_t) * tiles, cudaMemcpyHostToDevice, s), "batch upload")))
+        return st;
+    if ((st = cuda_err(cudaStreamSynchronize(s), "batch upload"))) return st;  // host vectors go out of scope
+    b->ntiles = tiles;
+    b->smem = smem;
+    if (smem > 48 * 1024 &&
+        (st = cuda_err(cudaFuncSetAttribute(k_batch, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem), "batch smem")))
+        return st;
+    int per_sm = 0;
+    if ((st = cuda_err(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch, BT_THREADS, smem), "batch occupancy")))
+        return st;
+    per_sm = std::max(per_sm, 1);
+    b->grid = (int)std::max<int64_t>(1, std::min<int64_t>(tiles, (int64_t)per_sm * b->sms));
+    b->finalized = true;
+    return IONP_OK;
+}
+
+int32_t enqueue_run(IonpBatch* b, cudaStream_t s) {
+    int32_t st;
+    if ((st = cuda_err(cudaMemsetAsync(b->d_next, 0, sizeof(unsigned long long), s), "batch reset"))) return st;
+    if ((st = cuda_err(cudaMemsetAsync(b->d_flags, 0, sizeof(uint32_t) * std::max<size_t>(b->calls.size(), 1), s), "batch reset")))
+        return st;
+    if (b->arrive_bytes && (st = cuda_err(cudaMemsetAsync(b->d_arrive, 0, b->arrive_bytes, s), "batch reset"))) return st;
+    if (b->ntiles == 0) return IONP_OK;
+    k_batch<<<b->grid, BT_THREADS, b->smem, s>>>(b->d_calls, b->d_tile_call, b->ntiles, b->d_next);
+    count_launch();
+    return cuda_err(cudaGetLastError(), "batch launch");
+}
+
+}  // namespace
+
+extern "C" {
+
+int32_t ionp_schedule_from_index(int32_t idx, IonpSchedule* s) {
+    if (!s || idx < 0 || idx >= IONP_NUM_SCHEDULES) return set_err(IONP_ERR_INVALID, "schedule index out of range");
+    static const int BT[4] = {128, 256, 512, 1024}, VW[3] = {1, 2, 4}, EPT[2] = {1, 4}, SP[2] = {1, 2};
+    s->block_tile = BT[idx / 12];
+    s->vec_width = VW[(idx / 4) % 3];
+    s->elems_per_thread = EPT[(idx / 2) % 2];
+    s->red_split = SP[idx % 2];
+    return IONP_OK;
+}
+
+int32_t ionp_batch_create(IonpBatch** out) {
+    if (!out) return set_err(IONP_ERR_INVALID, "NULL batch pointer");
+    IonpBatch* b = new IonpBatch();
+    int32_t st = cuda_err(cudaGetDevice(&b->device), "batch device");
+    if (!st) st = cuda_err(cudaDeviceGetAttribute(&b->sms, cudaDevAttrMultiProcessorCount, b->device), "batch device");
+    if (st) { delete b; return st; }
+    *out = b;
+    return IONP_OK;
+}
+
+int32_t ionp_batch_destroy(IonpBatch* b) {
+    if (!b) return IONP_OK;
+    cudaDeviceSynchronize();
+    release_device(b);
+    if (b->capture_stream) cudaStreamDestroy(b->capture_stream);
+    delete b;
+    return IONP_OK;
+}
+
+int32_t ionp_batch_add_binary(IonpBatch* b, int32_t op, const IonpArr* a, const IonpArr* bb, IonpArr* out,
+                              const IonpSchedule* sched, int32_t* call_id) {
+    int32_t st;
+    if (!b) return set_err(IONP_ERR_INVALID, "NULL batch");
+    if ((st = check_arr(a, "a")) || (st = check_arr(bb, "b")) || (st = check_arr(out, "out"))) return st;
+    if ((st = check_schedule(sched))) return st;
+    if (!(op == OP_ADD || op == OP_SUBTRACT || op == OP_MULTIPLY || op == OP_MAXIMUM || op == OP_LESS || op == OP_LOGICAL_AND))
+        return set_err(IONP_ERR_UNSUPPORTED, std::string("ufunc '") + op_name(op) + "' is not batched; call ionp_binary");
+    int cd, rd;
+    if ((st = binary_loop(op, a->dtype, bb->dtype, &cd, &rd))) return st;
+    if (out->dtype != rd) return set_err(IONP_ERR_UNSUPPORTED, "batched calls write the loop's result dtype; call ionp_binary");
+    const int nd = out->ndim;
+    if (numel(out) >= ((int64_t)1 << 31)) return set_err(IONP_ERR_UNSUPPORTED, "call too large for a batch; call ionp_binary");
+    MergeIn mi;
+    mi.nd = nd;
+    mi.nops = 3;
+    for (int i = 0; i < nd; ++i) { mi.shape[i] = out->shape[i]; mi.st[0][i] = out->strides[i]; }
+    if (!bcast_strides(a, nd, out->shape, mi.st[1]) || !bcast_strides(bb, nd, out->shape, mi.st[2]))
+        return set_err(IONP_ERR_BROADCAST, "operands could not be broadcast together with shapes " +
+                                               fmt_shape(a->shape, a->ndim) + " " + fmt_shape(bb->shape, bb->ndim) + " ");
+    MergeOut mo = merge_dims(mi);
+    if (mo.nd > 4) return set_err(IONP_ERR_UNSUPPORTED, "more than 4 merged dims; call ionp_binary");
+    BatchCall c;
+    memset(&c, 0, sizeof(c));
+    c.kind = BK_BINARY;
+    c.op = op;
+    c.cd = cd;
+    c.dta = a->dtype;
+    c.dtb = bb->dtype;
+    c.dto = out->dtype;
+    c.nd = mo.nd;
+    c.n = numel(out);
+    for (int i = 0; i < mo.nd; ++i) {
+        c.shape[i] = (int32_t)mo.shape[i];
+        c.div[i] = make_div((uint32_t)mo.shape[i]);
+        c.so[i] = mo.st[0][i];
+        c.sa[i] = mo.st[1][i];
+        c.sb[i] = mo.st[2][i];
+    }
+    c.a = elem_ptr(a);
+    c.b = elem_ptr(bb);
+    c.o = (void*)elem_ptr(out);
+    if (mo.nd == 1 && mo.st[0][0] == 1 && a->dtype == cd && bb->dtype == cd && out->dtype == rd) {
+        bool a_ok = mo.st[1][0] == 1 || mo.st[1][0] == 0, b_ok = mo.st[2][0] == 1 || mo.st[2][0] == 0;
+        bool al = (uintptr_t)c.o % 16 == 0 && (mo.st[1][0] == 0 || (uintptr_t)c.a % 16 == 0) &&
+                  (mo.st[2][0] == 0 || (uintptr_t)c.b % 16 == 0);
+        if (a_ok && b_ok && al) {
+            c.vec = 1;
+            c.a_sc = mo.st[1][0] == 0;
+            c.b_sc = mo.st[2][0] == 0;
+        }
+    }
+    c.user_id = (int32_t)b->calls.size();
+    IonpSchedule s;
+    if (sched) s = *sched; else set_default_schedule(&s);
+    b->calls.push_back(c);
+    b->sched.push_back(s);
+    IonpBatch::Orig o;
+    memset(&o, 0, sizeof(o));
+    o.kind = BK_BINARY; o.op = op; o.a = *a; o.b = *bb; o.out = *out;
+    b->orig.push_back(o);
+    b->finalized = false;
+    if (call_id) *call_id = c.user_id;
+    return IONP_OK;
+}
+
+int32_t ionp_batch_add_reduce(IonpBatch* b, int32_t op, const IonpArr* a, int32_t axis, int32_t keepdims, IonpArr* out,
+                              const IonpSchedule* sched, int32_t* call_id) {
+    int32_t st;
+    if (!b) return set_err(IONP_ERR_INVALID, "NULL batch");
+    if ((st = check_arr(a, "a")) || (st = check_arr(out, "out"))) return st;
+    if ((st = check_schedule(sched))) return st;
+    if (op != OP_ADD && op != OP_MAXIMUM)
+        return set_err(IONP_ERR_UNSUPPORTED, std::string("ufunc '") + op_name(op) + "'.reduce is not batched; call ionp_reduce");
+    const int nd = a->ndim;
+    if (nd == 0 || axis < 0 || axis >= nd) return set_err(IONP_ERR_AXIS, "batched reductions take one normalized axis");
+    if (!c_contiguous(a) || !c_contiguous(out))
+        return set_err(IONP_ERR_UNSUPPORTED, "batched reductions need C-contiguous input and output; call ionp_reduce");
+    int cd;
+    if ((st = reduce_cd(op, a->dtype, &cd))) return st;
+    if (a->dtype != cd && !(op == OP_ADD && (cd == DT_I64 || cd == DT_U64)))
+        return set_err(IONP_ERR_UNSUPPORTED, "the input would need a converted copy; call ionp_reduce");
+    if (out->dtype != cd) return set_err(IONP_ERR_UNSUPPORTED, "batched reductions write the compute dtype");
+    int64_t outer = 1, inner = 1, ext = a->shape[axis];
+    for (int i = 0; i < axis; ++i) outer *= a->shape[i];
+    for (int i = axis + 1; i < nd; ++i) inner *= a->shape[i];
+    const int want_nd = keepdims ? nd : nd - 1;
+    if (out->ndim != want_nd || numel(out) != outer * inner) return set_err(IONP_ERR_VALUE, "out has the wrong shape");
+    if (ext == 0) return set_err(IONP_ERR_UNSUPPORTED, "empty reduced extent; call ionp_reduce");
+    if (outer * inner >= ((int64_t)1 << 31) || numel(a) >= ((int64_t)1 << 40))
+        return set_err(IONP_ERR_UNSUPPORTED, "call too large for a batch; call ionp_reduce");
+    BatchCall c;
+    memset(&c, 0, sizeof(c));
+    c.op = op;
+    c.cd = cd;
+    c.dta = a->dtype;
+    c.dto = out->dtype;
+    c.a = elem_ptr(a);
+    c.o = (void*)elem_ptr(out);
+    c.n = outer * inner;
+    c.w = ext;
+    uint64_t seed = 0;
+    if (op == OP_ADD) {  // identity 0 of every add loop (add.reduce seeds with it)
+        c.has_seed = 1;
+        if (cd == DT_F16) seed = 0;
+        c.seed = seed;
+    }
+    // the reduced axis is the pairwise "wide" run (float add) / the row
+    // kernel's run when everything after it has extent 1; otherwise it folds
+    // sequentially per output (ufunc.rs:6658-6806, sequential_group 6546)
+    if (inner == 1) {
+        c.kind = BK_ROW;
+        c.rs = 1;
+        c.ostride = ext;
+    } else {
+        c.kind = BK_COL;
+        c.rs = inner;
+        c.inner = inner;
+        c.ostride = ext * inner;
+        c.idiv = make_div((uint32_t)inner);
+    }
+    c.user_id = (int32_t)b->calls.size();
+    IonpSchedule s;
+    if (sched) s = *sched; else set_default_schedule(&s);
+    b->calls.push_back(c);
+    b->sched.push_back(s);
+    IonpBatch::Orig o;
+    memset(&o, 0, sizeof(o));
+    o.kind = c.kind; o.op = op; o.a = *a; o.out = *out; o.axis = axis; o.keepdims = keepdims;
+    b->orig.push_back(o);
+    b->finalized = false;
+    if (call_id) *call_id = c.user_id;
+    return IONP_OK;
+}
+
+int32_t ionp_batch_set_schedule(IonpBatch* b, int32_t call, const IonpSchedule* sched) {
+    int32_t st;
+    if (!b || !sched || call < 0 || call >= (int32_t)b->calls.size()) return set_err(IONP_ERR_INVALID, "bad call index");
+    if ((st = check_schedule(sched))) return st;
+    b->sched[call] = *sched;
+    b->finalized = false;
+    return IONP_OK;
+}
+
+int32_t ionp_batch_finalize(IonpBatch* b, IonpStream stream) {
+    if (!b) return set_err(IONP_ERR_INVALID, "NULL batch");
+    return upload_and_plan(b, (cudaStream_t)stream);
+}
+
+int32_t ionp_batch_run(IonpBatch* b, int32_t use_graph, IonpStream stream) {
+    int32_t st;
+    if (!b) return set_err(IONP_ERR_INVALID, "NULL batch");
+    cudaStream_t s = (cudaStream_t)stream;
+    if (!b->finalized && (st = upload_and_plan(b, s))) return st;
+    if (!use_graph) return enqueue_run(b, s);
+    if (!b->gexec) {
+        if (!b->capture_stream &&
+            (st = cuda_err(cudaStreamCreateWithFlags(&b->capture_stream, cudaStreamNonBlocking), "capture stream")))
+            return st;
+        if ((st = cuda_err(cudaStreamBeginCapture(b->capture_stream, cudaStreamCaptureModeThreadLocal), "begin capture")))
+            return st;
+        int32_t est = enqueue_run(b, b->capture_stream);
+        cudaGraph_t g = nullptr;
+        cudaError_t e = cudaStreamEndCapture(b->capture_stream, &g);
+        if (est) { if (g) cudaGraphDestroy(g); return est; }
+        if ((st = cuda_err(e, "end capture"))) return st;
+        b->graph = g;
+        if ((st = cuda_err(cudaGraphInstantiate(&b->gexec, g, 0), "graph instantiate"))) return st;
+    }
+    return cuda_err(cudaGraphLaunch(b->gexec, s), "graph launch");
+}
+
+int32_t ionp_batch_run_per_call(IonpBatch* b, IonpStream stream) {
+    if (!b) return set_err(IONP_ERR_INVALID, "NULL batch");
+    for (size_t i = 0; i < b->orig.size(); ++i) {
+        IonpBatch::Orig& o = b->orig[i];
+        int32_t st;
+        if (o.kind == BK_BINARY) st = ionp_binary(o.op, &o.a, &o.b, &o.out, nullptr, nullptr, stream);
+        else {
+            int32_t ax = o.axis;
+            st = ionp_reduce(o.op, &o.a, &ax, 1, o.keepdims, -1, nullptr, nullptr, &o.out, stream);
+        }
+        if (st) return st;
+    }
+    return IONP_OK;
+}
+
+int32_t ionp_batch_fpe(IonpBatch* b, uint32_t* words, IonpStream stream) {
+    if (!b || !words) return set_err(IONP_ERR_INVALID, "bad arguments");
+    if (!b->finalized) return set_err(IONP_ERR_INVALID, "batch has not run");
+    cudaStream_t s = (cudaStream_t)stream;
+    int32_t st = cuda_err(cudaMemcpyAsync(words, b->d_flags, sizeof(uint32_t) * b->calls.size(), cudaMemcpyDeviceToHost, s), "fpe read");
+    if (st) return st;
+    return cuda_err(cudaStreamSynchronize(s), "fpe read");
+}
+
+int32_t ionp_batch_info(IonpBatch* b, int64_t* info) {
+    if (!b || !info) return set_err(IONP_ERR_INVALID, "bad arguments");
+    info[0] = (int64_t)b->calls.size();
+    info[1] = b->ntiles;
+    info[2] = b->grid;
+    info[3] = (int64_t)b->smem;
+    int64_t bytes = 0;
+    for (const BatchCall& c : b->calls) {
+        if (c.kind == BK_BINARY) {
+            const IonpBatch::Orig& o = b->orig[c.user_id];
+            bytes += numel(&o.a) * dt_size(c.dta) + numel(&o.b) * dt_size(c.dtb) + c.n * dt_size(c.dto);
+        } else {
+            bytes += c.n * c.w * dt_size(c.dta) + c.n * dt_size(c.dto);
+        }
+    }
+    info[4] = bytes;
+    return IONP_OK;
+}
+
+// Device time of one call of the batch under each of the given schedules:
+// the call alone is run `reps` times back to back as its own queue, between
+// two events, after one untimed run.
+int32_t ionp_batch_time_call(IonpBatch* b, int32_t call, int32_t nsched, const IonpSchedule* scheds, int32_t reps,
+                             float* us_out, IonpStream stream) {
+    int32_t st = IONP_OK;
+    if (!b || call < 0 || call >= (int32_t)b->calls.size() || nsched <= 0 || !scheds || !us_out || reps <= 0)
+        return set_err(IONP_ERR_INVALID, "bad arguments");
+    cudaStream_t s = (cudaStream_t)stream;
+    if (!b->finalized && (st = upload_and_plan(b, s))) return st;
+    if (!b->d_one) {
+        b->d_one = (BatchCall*)scratch_alloc(sizeof(BatchCall), s);
+        if (!b->d_one) return IONP_ERR_OOM;
+    }
+    cudaEvent_t e0, e1;
+    if ((st = cuda_err(cudaEventCreate(&e0), "time events"))) return st;
+    if ((st = cuda_err(cudaEventCreate(&e1), "time events"))) { cudaEventDestroy(e0); return st; }
+    for (int k = 0; k < nsched; ++k) {
+        if ((st = check_schedule(&scheds[k]))) break;
+        BatchCall c = b->calls[call];
+        tile_call(c, scheds[k]);
+        c.tile0 = 0;
+        c.flags = b->d_flags + c.user_id;
+        // tile -> call map of a one-call queue: all zeros
+        if (c.ntiles > b->one_cap) {
+            if (b->d_one_map) scratch_free(b->d_one_map, s);
+            b->one_cap = std::max<int64_t>(c.ntiles, 4096);
+            b->d_one_map = (int32_t*)scratch_alloc(sizeof(int32_t) * b->one_cap, s);
+            if (!b->d_one_map) { b->one_cap = 0; st = IONP_ERR_OOM; break; }
+            if ((st = cuda_err(cudaMemsetAsync(b->d_one_map, 0, sizeof(int32_t) * b->one_cap, s), "time map"))) break;
+        }
+        void* part = nullptr;
+        if (c.kind != BK_BINARY && c.split == 2) {
+            part = scratch_alloc((size_t)c.n * 20, s);
+            if (!part) { st = IONP_ERR_OOM; break; }
+            c.partial = part;
+            c.arrive = (uint32_t*)((char*)part + (size_t)c.n * 16);
+        }
+        const size_t smem = row_smem(c);
+        if (smem > 48 * 1024 &&
+            (st = cuda_err(cudaFuncSetAttribute(k_batch, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem), "time smem")))
+            break;
+        int per_sm = 1;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch, BT_THREADS, smem);
+        const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(c.ntiles, (int64_t)std::max(per_sm, 1) * b->sms));
+        if ((st = cuda_err(cudaMemcpyAsync(b->d_one, &c, sizeof(BatchCall), cudaMemcpyHostToDevice, s), "time upload"))) break;
+        auto one = [&]() {
+            cudaMemsetAsync(b->d_next, 0, 8, s);
+            if (c.arrive) cudaMemsetAsync(c.arrive, 0, (size_t)c.n * 4, s);
+            if (c.ntiles) k_batch<<<grid, BT_THREADS, smem, s>>>(b->d_one, b->d_one_map, c.ntiles, b->d_next);
+            count_launch();
+        };
+        one();
+        cudaEventRecord(e0, s);
+        for (int r = 0; r < reps; ++r) one();
+        cudaEventRecord(e1, s);
+        // the host copy of the descriptor and the split scratch stay alive
+        // until the runs are done
+        st = cuda_err(cudaEventSynchronize(e1), "time sync");
+        if (part) scratch_free(part, s);
+        if (st) break;
+        float ms = 0;
+        cudaEventElapsedTime(&ms, e0, e1);
+        us_out[k] = ms * 1000.0f / reps;
+        if ((st = cuda_err(cudaGetLastError(), "time launch"))) break;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    return st;
+}
+
+}  // extern "C"

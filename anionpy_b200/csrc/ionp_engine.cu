@@ -472,20 +472,6 @@ FlagWord::~FlagWord() {
 // ===========================================================================
 // element-wise planning
 // ===========================================================================
-namespace {
-
-struct MergeIn {
-    int nd;
-    int64_t shape[IONP_MAX_DIMS];
-    int nops;                       // operands incl. output (output first)
-    int64_t st[4][IONP_MAX_DIMS];
-};
-struct MergeOut {
-    int nd;
-    int64_t shape[IONP_MAX_DIMS];
-    int64_t st[4][IONP_MAX_DIMS];
-};
-
 // Drop unit dims, order by |output stride| (outermost first), and merge
 // neighbours whose strides chain for every operand.
 MergeOut merge_dims(const MergeIn& in) {
@@ -521,6 +507,8 @@ MergeOut merge_dims(const MergeIn& in) {
     }
     return r;
 }
+
+namespace {
 
 // Whether the reference's flat `x[i % len_x]` pairing (fpe.rs) equals true
 // broadcasting for operand `a` against the broadcast shape: a's shape must be

@@ -33,7 +33,9 @@ std::set<int64_t> seg_lengths(int64_t n, int K) {
     }
     return cur;
 }
-int tpr_for(int64_t w) { return w < 8 ? 1 : w <= PW_BLOCK ? 8 : w <= 2048 ? 32 : 256; }
+// threads per run: one thread sums a run of one leaf block, a warp a run of
+// up to 16 blocks, a whole CTA anything longer
+int tpr_for(int64_t w) { return w <= PW_BLOCK ? 1 : w <= 2048 ? 32 : 256; }
 
 struct Dim { int64_t n, st, ost, mst; };
 
@@ -100,7 +102,7 @@ int32_t run_row(RedDesc& d, cudaStream_t s) {
     int tpr = tpr_for(maxlen);
     size_t acc = (d.cd == DT_F16 && d.op == OP_ADD) ? 4 : (size_t)dt_bytes(d.cd);
     int groups = RED_THREADS / tpr;
-    size_t nslots = tpr >= 16 ? ((size_t)1 << D) : 1;
+    size_t nslots = tpr >= 32 ? ((size_t)1 << D) : 1;
     size_t smem = (size_t)groups * nslots * (acc + 1) + 16;
     d.K = K;
     d.D = D;

@@ -39,6 +39,22 @@ inline const char* elem_ptr(const IonpArr* a) {
 // broadcast_strides_to (shape.rs:113): strides of `a` viewed with `shape`
 bool bcast_strides(const IonpArr* a, int nd, const int64_t* shape, int64_t* out);
 
+// Dim merging of an element-wise call: up to 4 operands (output first) over
+// one shape; drops unit dims, orders dims by |output stride| (outermost
+// first) and merges neighbours whose strides chain for every operand.
+struct MergeIn {
+    int nd;
+    int64_t shape[IONP_MAX_DIMS];
+    int nops;
+    int64_t st[4][IONP_MAX_DIMS];
+};
+struct MergeOut {
+    int nd;
+    int64_t shape[IONP_MAX_DIMS];
+    int64_t st[4][IONP_MAX_DIMS];
+};
+MergeOut merge_dims(const MergeIn& in);
+
 // element-wise cast/copy of a into out with an optional bool mask
 int32_t cast_impl(const IonpArr* a, IonpArr* out, const IonpArr* where, cudaStream_t s);
 

@@ -16,14 +16,15 @@
 //    (sequential_group_ordered, ufunc.rs:6583).
 //
 // Kernels:
-//  k_red_row   : one output per thread group; the group's elements form one
-//                strided run. The pairwise tree is rebuilt on the device:
-//                every group of 8 threads ("octet") locates a leaf block by
-//                descending the split tree from the root, sums it with the 8
-//                accumulators, and parks the result in a shared-memory slot
-//                array laid out as a perfect binary tree (a leaf at depth d
-//                with path p sits at slot p << (D - d)); the tree is then
-//                combined level by level, left operand first. Associative
+//  k_red_row   : one output per thread group (1, 32 or 256 threads); the
+//                group's elements form one strided run. The pairwise tree is
+//                rebuilt on the device: each thread locates leaf blocks by
+//                descending the split tree from the root, sums each with the
+//                8 accumulators (16-byte vector loads on contiguous runs),
+//                and parks the result in a shared-memory slot array laid out
+//                as a perfect binary tree (a leaf at depth d with path p sits
+//                at slot p << (D - d)); the tree is then combined level by
+//                level, left operand first. Associative
 //                ops (int add, max, bitwise, ...) reuse the same kernel: any
 //                order-preserving bracketing gives identical bits for them.
 //                Runs longer than one CTA's segment are cut at a fixed tree
@@ -110,6 +111,9 @@ template <int OP, int CD, bool CASTLD = false> struct RPol {
     static constexpr int AD = F16W ? DT_F32 : CD;
     typedef typename DT<CD>::T T;
     typedef typename DT<AD>::T A;
+    // 8 consecutive elements load as one or two 16-byte vectors: plain 4- and
+    // 8-byte element types, and float16 widened to float32 after the load
+    static constexpr bool VEC8 = !CASTLD && (F16W || sizeof(T) == 4 || sizeof(T) == 8);
     static __device__ __forceinline__ A fold(A x, A y) { return BinOp<OP, AD>::apply(x, y); }
     static __device__ __forceinline__ A load(const void* p, int64_t e, int sdt) {
         if constexpr (CASTLD) return load_int_widen<CD>(p, e, sdt);
@@ -163,53 +167,131 @@ __device__ __forceinline__ void seg_of(int64_t n, int K, int64_t path, int64_t* 
     *len = l;
 }
 
-// Sum one leaf block [off, off+len) (len <= 128, len >= 8) with one octet.
-// Returns the octet's combined value in lane 0 of the octet (lane j of the
-// octet holds accumulator j before the combine).
+// Eight consecutive run elements [e, e+8) as accumulator values, loaded as
+// 16-byte vectors (the caller checked alignment).
 template <class P>
-__device__ __forceinline__ typename P::A leaf_octet(const void* p, int sdt, int64_t base, int64_t ws, int64_t off, int64_t len, int j) {
+__device__ __forceinline__ void load8_vec(const void* pa, int64_t e, typename P::A (&x)[8]) {
+    typedef typename P::T T;
+    if constexpr (P::F16W) {
+        uint4 u = __ldg(reinterpret_cast<const uint4*>(reinterpret_cast<const h16*>(pa) + e));
+        h16 h[8];
+        memcpy(h, &u, 16);
+#pragma unroll
+        for (int k = 0; k < 8; ++k) x[k] = h2f(h[k]);
+    } else if constexpr (sizeof(T) == 4) {
+        const uint4* q = reinterpret_cast<const uint4*>(reinterpret_cast<const T*>(pa) + e);
+        uint4 u0 = __ldg(q), u1 = __ldg(q + 1);
+        memcpy(&x[0], &u0, 16);
+        memcpy(&x[4], &u1, 16);
+    } else {
+        const uint4* q = reinterpret_cast<const uint4*>(reinterpret_cast<const T*>(pa) + e);
+        uint4 u0 = __ldg(q), u1 = __ldg(q + 1), u2 = __ldg(q + 2), u3 = __ldg(q + 3);
+        memcpy(&x[0], &u0, 16);
+        memcpy(&x[2], &u1, 16);
+        memcpy(&x[4], &u2, 16);
+        memcpy(&x[6], &u3, 16);
+    }
+}
+
+// One thread sums the leaf block [off, off+len) (len <= 128) of a run with
+// pairwise_sum's leaf loop (ufunc.rs:6416-6448): fewer than 8 elements fold
+// in order; otherwise 8 interleaved accumulators (r[k] takes elements
+// k, k+8, ...), combined ((r0+r1)+(r2+r3))+((r4+r5)+(r6+r7)), then the
+// len % 8 tail added in order. Float max/min (P::CHUNK) fold strictly left
+// to right, which their first-NaN rule needs. Contiguous runs load 8
+// elements per 16-byte vector pair.
+template <class P>
+__device__ __forceinline__ typename P::A leaf_thread(const void* pa, int adt, int64_t base, int64_t ws, int64_t off,
+                                                     int64_t len) {
     typedef typename P::A A;
-    if constexpr (P::CHUNK) {
-        // lane j folds [j*len/8, (j+1)*len/8) in order (len >= 8: no lane is empty)
-        const int64_t b0 = off + (j * len) / 8, b1 = off + ((j + 1) * len) / 8;
-        A r = P::load(p, base + b0 * ws, sdt);
-        A x[15];
+    typedef typename P::T T;
+    const int64_t e0 = base + off * ws;
+    if constexpr (P::CHUNK && P::VEC8) {
+        // order-sensitive folds on contiguous runs: vector loads, strictly
+        // left-to-right fold
+        if (len >= 8 && ws == 1 && ((reinterpret_cast<uintptr_t>(pa) + (uint64_t)e0 * sizeof(T)) & 15) == 0) {
+            constexpr int GC = sizeof(T) == 8 ? 1 : 2;
+            const int64_t lim = len - len % 8;
+            A x0[8];
+            load8_vec<P>(pa, e0, x0);
+            A r = x0[0];
 #pragma unroll
-        for (int i = 0; i < 15; ++i)
-            if (b0 + 1 + i < b1) x[i] = P::load(p, base + (b0 + 1 + i) * ws, sdt);
+            for (int k = 1; k < 8; ++k) r = P::fold(r, x0[k]);
+            for (int64_t i = 8; i < lim; i += 8 * GC) {
+                A x[GC][8];
 #pragma unroll
-        for (int i = 0; i < 15; ++i)
-            if (b0 + 1 + i < b1) r = P::fold(r, x[i]);
-        const unsigned cmask = 0xFFu << ((threadIdx.x & 31) & ~7u);
+                for (int g = 0; g < GC; ++g)
+                    if (i + 8 * g < lim) load8_vec<P>(pa, e0 + i + 8 * g, x[g]);
 #pragma unroll
-        for (int s = 1; s < 8; s <<= 1) {
-            A other = __shfl_down_sync(cmask, r, s, 8);
-            if ((j & (2 * s - 1)) == 0) r = P::fold(r, other);
+                for (int g = 0; g < GC; ++g)
+                    if (i + 8 * g < lim) {
+#pragma unroll
+                        for (int k = 0; k < 8; ++k) r = P::fold(r, x[g][k]);
+                    }
+            }
+            for (int64_t i = lim; i < len; ++i) r = P::fold(r, P::load(pa, e0 + i, adt));
+            return r;
         }
+    }
+    if (P::CHUNK || len < 8) {
+        A r = P::load(pa, e0, adt);
+        int64_t i = 1;
+        for (; i + 8 <= len; i += 8) {
+            A x[8];
+#pragma unroll
+            for (int k = 0; k < 8; ++k) x[k] = P::load(pa, e0 + (i + k) * ws, adt);
+#pragma unroll
+            for (int k = 0; k < 8; ++k) r = P::fold(r, x[k]);
+        }
+        for (; i < len; ++i) r = P::fold(r, P::load(pa, e0 + i * ws, adt));
         return r;
     }
     const int64_t lim = len - len % 8;
-    A r = P::load(p, base + (off + j) * ws, sdt);
-    A x[15];
+    A r[8];
+    bool vec = false;
+    if constexpr (P::VEC8) vec = ws == 1 && ((reinterpret_cast<uintptr_t>(pa) + (uint64_t)e0 * sizeof(T)) & 15) == 0;
+    if (vec) {
+        if constexpr (P::VEC8) {
+            // 64 bytes of loads in flight per chunk: two 8-element groups of
+            // 4-byte (or widened 2-byte) elements, one of 8-byte elements
+            constexpr int GC = sizeof(T) == 8 ? 1 : 2;
+            load8_vec<P>(pa, e0, r);
+            for (int64_t i = 8; i < lim; i += 8 * GC) {
+                A x[GC][8];
 #pragma unroll
-    for (int i = 0; i < 15; ++i) {
-        int64_t e = off + 8 * (i + 1) + j;
-        if (8 * (i + 1) < lim) x[i] = P::load(p, base + e * ws, sdt);
-    }
+                for (int g = 0; g < GC; ++g)
+                    if (i + 8 * g < lim) load8_vec<P>(pa, e0 + i + 8 * g, x[g]);
 #pragma unroll
-    for (int i = 0; i < 15; ++i)
-        if (8 * (i + 1) < lim) r = P::fold(r, x[i]);
-    // ((r0+r1)+(r2+r3))+((r4+r5)+(r6+r7)): lower lane is the left operand
-    const unsigned mask = 0xFFu << ((threadIdx.x & 31) & ~7u);
+                for (int g = 0; g < GC; ++g)
+                    if (i + 8 * g < lim) {
 #pragma unroll
-    for (int s = 1; s < 8; s <<= 1) {
-        A other = __shfl_down_sync(mask, r, s, 8);
-        if ((j & (2 * s - 1)) == 0) r = P::fold(r, other);
+                        for (int k = 0; k < 8; ++k) r[k] = P::fold(r[k], x[g][k]);
+                    }
+            }
+        }
+    } else {
+        constexpr int GS = sizeof(A) == 8 ? 1 : 2;
+#pragma unroll
+        for (int k = 0; k < 8; ++k) r[k] = P::load(pa, e0 + k * ws, adt);
+        for (int64_t i = 8; i < lim; i += 8 * GS) {
+            A x[GS][8];
+#pragma unroll
+            for (int g = 0; g < GS; ++g)
+                if (i + 8 * g < lim) {
+#pragma unroll
+                    for (int k = 0; k < 8; ++k) x[g][k] = P::load(pa, e0 + (i + 8 * g + k) * ws, adt);
+                }
+#pragma unroll
+            for (int g = 0; g < GS; ++g)
+                if (i + 8 * g < lim) {
+#pragma unroll
+                    for (int k = 0; k < 8; ++k) r[k] = P::fold(r[k], x[g][k]);
+                }
+        }
     }
-    if (j == 0) {
-        for (int64_t i = lim; i < len; ++i) r = P::fold(r, P::load(p, base + (off + i) * ws, sdt));
-    }
-    return r;
+    A res = P::fold(P::fold(P::fold(r[0], r[1]), P::fold(r[2], r[3])), P::fold(P::fold(r[4], r[5]), P::fold(r[6], r[7])));
+    for (int64_t i = lim; i < len; ++i) res = P::fold(res, P::load(pa, e0 + i * ws, adt));
+    return res;
 }
 
 // Barrier over one TPR-thread group (a CTA-wide barrier when TPR > 32).
@@ -220,56 +302,39 @@ template <int TPR> __device__ __forceinline__ void group_sync() {
 }
 
 // One output group of TPR threads reduces the run [seg_off, seg_off+n) of
-// output row `base` with the pairwise tree; result valid in the group's
-// thread 0. `slots`/`valid` are this group's 2^D shared-memory slots.
+// output row `base` with the pairwise tree, one leaf per thread: every
+// thread takes the leaf blocks that start in its 64-element candidate
+// windows (each leaf, 64..128 elements long, starts in exactly one window),
+// sums it with leaf_thread and parks it in the perfect-binary-tree slot
+// array; the slots are then combined level by level, left operand first.
 template <class P, int TPR>
-__device__ typename P::A group_tree(const RedDesc& d, int64_t base, int64_t seg_off, int64_t n, int D,
-                                    typename P::A* slots, uint8_t* valid, int t) {
+__device__ typename P::A group_tree_t(const void* pa, int adt, int64_t aws, int64_t base, int64_t seg_off, int64_t n,
+                                      int D, typename P::A* slots, uint8_t* valid, int t) {
     typedef typename P::A A;
-    const int ws = 0;
-    (void)ws;
-    if (n < 8) {
-        A r{};
-        if (t == 0 && n > 0) {
-            r = P::load(d.a, base + seg_off * d.ws, d.adt);
-            for (int64_t i = 1; i < n; ++i) r = P::fold(r, P::load(d.a, base + (seg_off + i) * d.ws, d.adt));
-        }
-        return r;
-    }
-    const int oct = t >> 3, j = t & 7;
-    constexpr int NOCT = TPR / 8;
     if (n <= PW_BLOCK) {
         A r{};
-        if (oct == 0) r = leaf_octet<P>(d.a, d.adt, base, d.ws, seg_off, n, j);
+        if (t == 0 && n > 0) r = leaf_thread<P>(pa, adt, base, aws, seg_off, n);
         return r;
     }
     const int nslots = 1 << D;
     for (int s = t; s < nslots; s += TPR) valid[s] = 0;
     group_sync<TPR>();
     const int64_t ncand = (n + 63) / 64;
-    for (int64_t c0 = 0; c0 < ncand; c0 += NOCT) {
-        int64_t c = c0 + oct;
+    for (int64_t c = t; c < ncand; c += TPR) {
+        const int64_t m = c * 64;
         int64_t off = 0, len = n, path = 0;
         int depth = 0;
-        bool own = false;
-        if (c < ncand) {
-            int64_t m = c * 64;
-            while (len > PW_BLOCK) {
-                int64_t n2 = pw_split(len);
-                path <<= 1;
-                depth++;
-                if (m < off + n2) len = n2; else { off += n2; len -= n2; path |= 1; }
-            }
-            own = off > m - 64;
+        while (len > PW_BLOCK) {
+            int64_t n2 = pw_split(len);
+            path <<= 1;
+            depth++;
+            if (m < off + n2) len = n2; else { off += n2; len -= n2; path |= 1; }
         }
-        // octets are warp-aligned; the whole octet agrees on `own`
-        if (own) {
-            A r = leaf_octet<P>(d.a, d.adt, base, d.ws, seg_off + off, len, j);
-            if (j == 0) {
-                int s = (int)(path << (D - depth));
-                slots[s] = r;
-                valid[s] = 1;
-            }
+        if (off > m - 64) {
+            A r = leaf_thread<P>(pa, adt, base, aws, seg_off + off, len);
+            int s = (int)(path << (D - depth));
+            slots[s] = r;
+            valid[s] = 1;
         }
     }
     group_sync<TPR>();
@@ -285,14 +350,14 @@ __device__ typename P::A group_tree(const RedDesc& d, int64_t base, int64_t seg_
 
 // ROW kernel. Tasks = nout x 2^K; each TPR-thread group takes one task.
 template <int OP, int CD, int TPR, bool CASTLD>
-__global__ void __launch_bounds__(RED_THREADS) k_red_row(RedDesc d) {
+__global__ void __launch_bounds__(RED_THREADS, 4) k_red_row(RedDesc d) {
     typedef RPol<OP, CD, CASTLD> P;
     typedef typename P::A A;
     typedef typename P::T T;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     constexpr int GROUPS = RED_THREADS / TPR;
     const int g = threadIdx.x / TPR, t = threadIdx.x % TPR;
-    const int nslots = TPR >= 16 ? (1 << d.D) : 1;
+    const int nslots = TPR >= 32 ? (1 << d.D) : 1;
     A* slots = reinterpret_cast<A*>(smem_raw) + (size_t)g * nslots;
     uint8_t* valid = reinterpret_cast<uint8_t*>(reinterpret_cast<A*>(smem_raw) + (size_t)GROUPS * nslots) + (size_t)g * nslots;
     const int64_t nseg = (int64_t)1 << d.K;
@@ -308,10 +373,12 @@ __global__ void __launch_bounds__(RED_THREADS) k_red_row(RedDesc d) {
         seg_of(d.w, d.K, sg, &soff, &slen);
         if (!live) slen = 0;
         A r{};
-        if constexpr (TPR > 32) {
-            r = group_tree<P, TPR>(d, in_off, soff, slen, d.D, slots, valid, t);
+        if constexpr (TPR == 1) {
+            if (slen > 0) r = leaf_thread<P>(d.a, d.adt, in_off, d.ws, soff, slen);
+        } else if constexpr (TPR > 32) {
+            r = group_tree_t<P, TPR>(d.a, d.adt, d.ws, in_off, soff, slen, d.D, slots, valid, t);
         } else {
-            if (slen > 0) r = group_tree<P, TPR>(d, in_off, soff, slen, d.D, slots, valid, t);
+            if (slen > 0) r = group_tree_t<P, TPR>(d.a, d.adt, d.ws, in_off, soff, slen, d.D, slots, valid, t);
         }
         if (live && t == 0) {
             if (d.K == 0) store_cast<CD>(d.o, out_off, d.odt, P::finish(r, d.has_seed, d.seed));
@@ -369,7 +436,7 @@ __global__ void __launch_bounds__(RED_THREADS) k_red_col(RedDesc d) {
         for (int64_t done = 0; done < total; done += rn_in) {
             const int64_t b0 = base + outer_off;
             int64_t j = 0;
-            constexpr int U = 8;
+            constexpr int U = 16;
             for (; j + U <= rn_in; j += U) {
                 T x[U];
 #pragma unroll
@@ -399,6 +466,88 @@ __global__ void __launch_bounds__(RED_THREADS) k_red_col(RedDesc d) {
             }
         }
         store_cast<CD>(d.o, out_off, d.odt, acc);
+    }
+}
+
+// 16-byte asynchronous global -> shared copies (cp.async, L2-only caching).
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+    unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N> __device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+// COL kernel, staged: one narrow axis, contiguous kept axis. A CTA owns the
+// outputs of one 128-byte column slice (32 float32 / 16 float64 columns);
+// all 256 threads stream 64-row stages of it into a 3-stage shared-memory
+// ring with cp.async while one warp folds each column sequentially in row
+// order (the narrow fold of ufunc.rs:6748-6795 / sequential_group). Two
+// stages are in flight while the third is folded, and seven such CTAs per
+// SM keep HBM busy even when the outputs are too few for one thread each
+// to hide the latency.
+constexpr int COLST_ROWS = 64;    // rows per stage
+constexpr int COLST_STAGES = 3;
+constexpr int COLST_CTAS = 7;     // resident CTAs per SM the kernel is sized for
+template <class T> constexpr int colst_cols() { return 128 / (int)sizeof(T); }
+template <class T> constexpr size_t colst_smem() { return (size_t)COLST_STAGES * COLST_ROWS * 128; }
+
+template <int OP, int CD>
+__global__ void __launch_bounds__(RED_THREADS, COLST_CTAS) k_red_col_staged(RedDesc d) {
+    typedef typename DT<CD>::T T;
+    constexpr int ES = (int)sizeof(T);
+    constexpr int VE = 16 / ES;                 // elements per 16-byte chunk
+    constexpr int COLS = colst_cols<T>();       // columns per CTA (one 128-byte slice)
+    constexpr int CPR = COLS / VE;              // chunks per row: 8
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T* buf = reinterpret_cast<T*>(smem_raw);
+    const int64_t ncols = d.kshape[0];
+    const int64_t rows = d.rshape[0];
+    const int64_t rstride = d.rst[0];
+    const T* a = reinterpret_cast<const T*>(d.a);
+    const int64_t nst = (rows + COLST_ROWS - 1) / COLST_ROWS;
+    const int64_t ntiles = (ncols + COLS - 1) / COLS;
+    for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        const int64_t c0 = tile * COLS;
+        auto issue = [&](int64_t st) {
+            if (st < nst) {
+                T* sb = buf + (st % COLST_STAGES) * COLST_ROWS * COLS;
+                for (int q = threadIdx.x; q < COLST_ROWS * CPR; q += RED_THREADS) {
+                    const int r = q / CPR, ch = q - r * CPR;
+                    const int64_t row = st * COLST_ROWS + r, col = c0 + (int64_t)ch * VE;
+                    if (row < rows && col < ncols) cp_async16(sb + r * COLS + ch * VE, a + row * rstride + col);
+                }
+            }
+            cp_async_commit();  // empty groups keep the group count uniform
+        };
+        for (int st = 0; st < COLST_STAGES - 1; ++st) issue(st);
+        T acc;
+        memcpy(&acc, &d.seed, sizeof(T));
+        bool have = d.has_seed != 0;
+        const int64_t my = c0 + threadIdx.x;
+        const bool owner = threadIdx.x < COLS && my < ncols;
+        for (int64_t st = 0; st < nst; ++st) {
+            issue(st + COLST_STAGES - 1);
+            cp_async_wait<COLST_STAGES - 1>();
+            __syncthreads();
+            if (owner) {
+                const T* sb = buf + (st % COLST_STAGES) * COLST_ROWS * COLS + threadIdx.x;
+                const int nr = (int)(rows - st * COLST_ROWS < COLST_ROWS ? rows - st * COLST_ROWS : COLST_ROWS);
+                int r = 0;
+                if (!have) { acc = sb[0]; have = true; r = 1; }
+                for (; r + 8 <= nr; r += 8) {
+                    T x[8];
+#pragma unroll
+                    for (int u = 0; u < 8; ++u) x[u] = sb[(r + u) * COLS];
+#pragma unroll
+                    for (int u = 0; u < 8; ++u) acc = BinOp<OP, CD>::apply(acc, x[u]);
+                }
+                for (; r < nr; ++r) acc = BinOp<OP, CD>::apply(acc, sb[r * COLS]);
+            }
+            __syncthreads();
+        }
+        if (owner) store_cast<CD>(d.o, my * d.kost[0], d.odt, acc);
     }
 }
 

@@ -73,7 +73,7 @@ std::set<int64_t> lengths_at(int64_t n, int K) {
     }
     return cur;
 }
-int threads_per_run(int64_t w) { return w < 8 ? 1 : w <= PW_BLOCK ? 8 : w <= 2048 ? 32 : 256; }
+int threads_per_run(int64_t w) { return w <= PW_BLOCK ? 1 : w <= 2048 ? 32 : 256; }
 
 bool identity_of(int op, int cd, uint64_t* out) {
     *out = 0;
@@ -239,7 +239,7 @@ extern "C" int32_t ionp_reduce_noalloc(int32_t op, const IonpArr* a, const int32
     for (int64_t l : lens) D = std::max(D, tree_depth(l));
     const int tpr = threads_per_run(*lens.rbegin());
     const int groups = RED_THREADS / tpr;
-    const size_t nslots = tpr >= 16 ? ((size_t)1 << D) : 1;
+    const size_t nslots = tpr >= 32 ? ((size_t)1 << D) : 1;
     const size_t smem = (size_t)groups * nslots * (acc + 1) + 16;
     d.K = K;
     d.D = D;

@@ -11,7 +11,6 @@ template <int OP, int CD, bool C>
 static cudaError_t row_t2(const RedDesc& d, int tpr, size_t smem, int grid, cudaStream_t s) {
     switch (tpr) {
         case 1: k_red_row<OP, CD, 1, C><<<grid, RED_THREADS, smem, s>>>(d); break;
-        case 8: k_red_row<OP, CD, 8, C><<<grid, RED_THREADS, smem, s>>>(d); break;
         case 32: k_red_row<OP, CD, 32, C><<<grid, RED_THREADS, smem, s>>>(d); break;
         default: {
             auto k = k_red_row<OP, CD, 256, C>;

@@ -10,10 +10,45 @@ static int seq_grid(int64_t nout, int threads) {
     return (int)g;
 }
 
+// The staged column kernel applies to one narrow axis over one contiguous
+// kept axis, 4- or 8-byte elements, 16-byte aligned rows.
+static bool col_staged_ok(const RedDesc& d, int es) {
+    if (d.adt != d.cd || (es != 4 && es != 8)) return false;
+    if (d.nr != 1 || d.nk != 1 || d.kst[0] != 1 || d.rst[0] <= 0) return false;
+    if (d.kshape[0] % (16 / es) != 0 || (d.rst[0] * es) % 16 != 0) return false;
+    if (reinterpret_cast<uintptr_t>(d.a) % 16 != 0) return false;
+    // with 64K or more outputs one thread per output already keeps enough
+    // loads in flight; the staged kernel pays off below that
+    return d.rshape[0] >= 64 && d.kshape[0] >= 128 / es && d.nout < 65536;
+}
+
+template <int OPV, int D>
+static cudaError_t col_staged(const RedDesc& d, cudaStream_t s) {
+    typedef typename DT<D>::T T;
+    const size_t smem = colst_smem<T>();
+    auto k = k_red_col_staged<OPV, D>;
+    cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    const int64_t tiles = (d.kshape[0] + colst_cols<T>() - 1) / colst_cols<T>();
+    const int64_t cap = 148LL * COLST_CTAS;
+    int grid = (int)(tiles < cap ? tiles : cap);
+    k<<<grid, RED_THREADS, smem, s>>>(d);
+    count_launch();
+    return cudaGetLastError();
+}
+
 template <int OPV>
 static cudaError_t col_op(const RedDesc& d, cudaStream_t s) {
     const bool castld = d.adt != d.cd;
     const int grid = seq_grid(d.nout, RED_THREADS);
+    if (col_staged_ok(d, dt_size(d.cd))) {
+#define IONP_STCASE(D)                                                                   \
+        case D:                                                                          \
+            if constexpr (red_any_valid(OPV, D) && (sizeof(typename DT<D>::T) >= 4))     \
+                return col_staged<OPV, D>(d, s);                                         \
+            break;
+        switch (d.cd) { IONP_DTS(IONP_STCASE) }
+#undef IONP_STCASE
+    }
 #define IONP_DTCASE(D)                                                                          \
     case D:                                                                                     \
         if constexpr (red_any_valid(OPV, D)) {                                                  \

@@ -282,6 +282,73 @@ class SweepItem:
 
 
 # ---------------------------------------------------------------------------
+# batched mixed stream: 10,000 small calls as one persistent kernel (+graph)
+# versus one default-schedule launch per call
+# ---------------------------------------------------------------------------
+def mixed_stream_bench(ap, L, steps, warmup, ncalls=10000, check_every=10, schedules=None):
+    from anionpy_b200 import _lib, workloads
+    calls, skipped = workloads.mixed_stream(ncalls=ncalls, seed=7)
+    pools = workloads.DevicePools(ap, pool_elems=1 << 22, seed=17)
+    b, hosts = workloads.build_batch(ap, calls, pools, keep_host=True)
+    L.ionp_device_synchronize()
+    e0, e1 = ctypes.c_void_p(), ctypes.c_void_p()
+    L.ionp_event_create(ctypes.byref(e0))
+    L.ionp_event_create(ctypes.byref(e1))
+
+    def timed(fn):
+        for _ in range(max(warmup, 1)):
+            fn()
+        L.ionp_device_synchronize()
+        L.ionp_event_record(e0, None)
+        for _ in range(steps):
+            fn()
+        L.ionp_event_record(e1, None)
+        ms = ctypes.c_float()
+        _lib.check(L.ionp_event_elapsed_ms(e0, e1, ctypes.byref(ms)))
+        return ms.value / steps
+
+    launches0 = _lib.launch_count()
+    t_per = timed(b.run_per_call)
+    per_call_launches = (_lib.launch_count() - launches0) / (max(warmup, 1) + steps)
+    want = [o.get() for o in b.outputs]
+    t_pers = timed(lambda: b.run(graph=False))
+    t_graph = timed(lambda: b.run(graph=True))
+    res = {"calls": len(calls), "skipped_bool_subtract": skipped, "bytes_per_run": b.info()["bytes"],
+           "tiles": b.info()["tiles"], "grid": b.info()["grid"],
+           "per_launch_ms": round(t_per, 3), "per_launch_kernels_per_run": per_call_launches,
+           "persistent_ms": round(t_pers, 3), "persistent_graph_ms": round(t_graph, 3),
+           "calls_per_s_per_launch": round(len(calls) / (t_per / 1e3)),
+           "calls_per_s_persistent_graph": round(len(calls) / (t_graph / 1e3)),
+           "speedup_graph_vs_per_launch": round(t_per / t_graph, 2),
+           "GB/s_persistent_graph": round(b.info()["bytes"] / (t_graph / 1e3) / 1e9, 1)}
+    if schedules is not None:
+        b.set_schedules(schedules)
+        t_learn = timed(lambda: b.run(graph=True))
+        res["learned_graph_ms"] = round(t_learn, 3)
+        res["speedup_learned_vs_per_launch"] = round(t_per / t_learn, 2)
+        res["calls_per_s_learned_graph"] = round(len(calls) / (t_learn / 1e3))
+    # parity: every batched output against the per-launch output, bit for
+    # bit; every `check_every`-th call also against the oracle
+    got = [o.get() for o in b.outputs]
+    bad = sum(int(g.tobytes() != w.tobytes()) for g, w in zip(got, want))
+    from oracle import oracle as O
+    bad_o = 0
+    checked_o = 0
+    for i in range(0, len(calls), check_every):
+        c, h = calls[i], hosts[i]
+        if c.kind == "binary":
+            ref = O.binary(c.op, h[0], h[1])[0]
+        else:
+            ref = np.asarray(O.reduce(c.op, h[0], axis=c.axis))
+        bad_o += int(ref.reshape(-1).tobytes() != got[i].reshape(-1).tobytes())
+        checked_o += 1
+    res["mismatches_vs_per_launch"] = bad
+    res["oracle_checked"] = checked_o
+    res["mismatches_vs_oracle"] = bad_o
+    return res, b
+
+
+# ---------------------------------------------------------------------------
 # clocks sampled during the timed region
 # ---------------------------------------------------------------------------
 class Clocks:
@@ -417,6 +484,7 @@ def main():
     ap_.add_argument("--no-reduce", action="store_true", help="skip the reduction cases")
     ap_.add_argument("--reduce-scale", type=int, default=1, help="divide the reductions' leading extent (small runs)")
     ap_.add_argument("--no-parity", action="store_true", help="skip the oracle checks after the timed region")
+    ap_.add_argument("--no-stream", action="store_true", help="skip the batched mixed stream")
     args = ap_.parse_args()
     if args.impl == "reference":
         return reference_arm(args)
@@ -500,7 +568,7 @@ def main():
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         total_ms = float(t.item())
     step_bytes = sum(it.nbytes for it in items)
-    value = step_bytes * args.steps * world / (total_ms / 1e3) / 1e9
+    value = step_bytes * args.steps * world / (total_ms / 1e3) / 1e9 if total_ms > 0 else 0.0
 
     # per-case achieved bandwidth and the dominant kernel's roofline
     per_case /= args.steps
@@ -508,8 +576,8 @@ def main():
     for it, ms in zip(items, per_case):
         gbs = it.nbytes / (ms / 1e3) / 1e9
         rows.append({"case": it.name, "ms": round(float(ms), 4), "GB/s": round(gbs, 1), "frac": round(gbs / hbm_peak, 3)})
-    dom = int(np.argmax(per_case))
-    head = ([r for r in rows if r["case"] == "add/float32/contig"] or [rows[0]])[0]
+    dom = int(np.argmax(per_case)) if len(items) else None
+    head = ([r for r in rows if r["case"] == "add/float32/contig"] or rows[:1] or [None])[0]
     sweep_ms = float(sum(per_case[i] for i, it in enumerate(items) if isinstance(it, SweepItem)))
     red_ms = float(sum(per_case[i] for i, it in enumerate(items) if isinstance(it, ReduceCase)))
     sweep_b = sum(it.nbytes for it in items if isinstance(it, SweepItem))
@@ -526,6 +594,10 @@ def main():
                 continue
             checked += 1
             mismatches += int(not ok)
+
+    mixed = None
+    if rank == 0 and not args.no_stream:
+        mixed, _ = mixed_stream_bench(ap, L, args.steps, args.warmup)
 
     # end-to-end through the public API with pinned host buffers
     e2e = None
@@ -558,9 +630,11 @@ def main():
                       "reduce": {"GB/s": round(red_b / (red_ms / 1e3) / 1e9, 1) if red_ms else None,
                                  "frac": round(red_b / (red_ms / 1e3) / 1e9 / hbm_peak, 3) if red_ms else None,
                                  "ms": round(red_ms, 3)}},
-            "roofline": {"bound": "hbm", "kernel": rows[dom]["case"], "achieved": rows[dom]["GB/s"], "peak": hbm_peak,
-                         "unit": "GB/s", "frac": rows[dom]["frac"], "traffic": None, "peak_kind": peak_kind,
-                         "headline_add_f32_contig": head},
+            "roofline": None if dom is None else
+            {"bound": "hbm", "kernel": rows[dom]["case"], "achieved": rows[dom]["GB/s"], "peak": hbm_peak,
+             "unit": "GB/s", "frac": rows[dom]["frac"], "traffic": None, "peak_kind": peak_kind,
+             "headline_add_f32_contig": head},
+            "mixed_stream": mixed,
             "cpu_baseline": cpu,
             "e2e": e2e,
             "gpu_launches": int(launches),

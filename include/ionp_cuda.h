@@ -170,6 +170,58 @@ int32_t ionp_reduce_noalloc(int32_t op, const IonpArr* a, const int32_t* axes, i
 int32_t ionp_argext(int32_t is_max, const IonpArr* a, int32_t axis, int32_t keepdims, IonpArr* out,
                     IonpStream stream);
 
+/* ---------------------------------------------------------------- batches */
+/* Many small calls as one persistent kernel over a device queue of call
+ * descriptors, captured in a CUDA graph. No counterpart in the reference,
+ * which runs each call on its own (ionp-py/src/lib.rs:9205 __call__,
+ * lib.rs:9959 reduce); every call computes exactly what ionp_binary /
+ * ionp_reduce compute for it.
+ *
+ * A schedule is a point of a 48-point space: block tile {128,256,512,1024} x
+ * vector width {1,2,4} (16-byte units) x elements per thread {1,4} x
+ * reduction split {1,2}. It changes how a call is cut into tiles and mapped
+ * to threads, never a result bit. Index order: block tile slowest, split
+ * fastest (ionp_schedule_from_index). */
+typedef struct IonpSchedule {
+    int32_t block_tile, vec_width, elems_per_thread, red_split;
+} IonpSchedule;
+#define IONP_NUM_SCHEDULES 48
+int32_t ionp_schedule_from_index(int32_t idx, IonpSchedule* s);
+
+typedef struct IonpBatch IonpBatch;
+int32_t ionp_batch_create(IonpBatch** b);
+int32_t ionp_batch_destroy(IonpBatch* b);
+/* Binary call: add, subtract, multiply, maximum, less, logical_and; any
+ * dtypes, broadcasting and strides (at most 4 merged dims, fewer than 2^31
+ * output elements). sched NULL = the default schedule. */
+int32_t ionp_batch_add_binary(IonpBatch* b, int32_t op, const IonpArr* a, const IonpArr* bb, IonpArr* out,
+                              const IonpSchedule* sched, int32_t* call_id);
+/* add.reduce / maximum.reduce over one axis of a C-contiguous array into a
+ * C-contiguous output of the compute dtype. */
+int32_t ionp_batch_add_reduce(IonpBatch* b, int32_t op, const IonpArr* a, int32_t axis, int32_t keepdims, IonpArr* out,
+                              const IonpSchedule* sched, int32_t* call_id);
+int32_t ionp_batch_set_schedule(IonpBatch* b, int32_t call, const IonpSchedule* sched);
+/* Plans the tiles and uploads the queue (run does it when needed). */
+int32_t ionp_batch_finalize(IonpBatch* b, IonpStream stream);
+/* Runs every call: one persistent kernel; use_graph=1 captures the run once
+ * in a CUDA graph and replays the graph afterwards. */
+int32_t ionp_batch_run(IonpBatch* b, int32_t use_graph, IonpStream stream);
+/* The same calls, one ionp_binary / ionp_reduce launch per call (default
+ * schedules): the baseline the batch is measured against. */
+int32_t ionp_batch_run_per_call(IonpBatch* b, IonpStream stream);
+/* FPE words (IONP_FPE_* bits) of every call of the last run, caller order.
+ * The batch pairs operands by broadcasting; for float multiply calls whose
+ * operands are not trailing-aligned the reference's detector pairs them by
+ * flat index, which ionp_binary reproduces and the batch does not. */
+int32_t ionp_batch_fpe(IonpBatch* b, uint32_t* words, IonpStream stream);
+/* info[0] calls, [1] tiles, [2] grid, [3] dynamic shared bytes,
+ * [4] algorithmic bytes of one run */
+int32_t ionp_batch_info(IonpBatch* b, int64_t* info);
+/* Device microseconds of one call run alone under each schedule (the
+ * autotuner's measurement): reps back-to-back runs between two events. */
+int32_t ionp_batch_time_call(IonpBatch* b, int32_t call, int32_t nsched, const IonpSchedule* scheds, int32_t reps,
+                             float* us_out, IonpStream stream);
+
 /* ---------------------------------------------------------------- memory */
 /* Caching device allocator (the device counterpart of Buffer's Vec<T>,
  * ionp-core/src/buffer.rs:18): size-classed free lists, stream-ordered reuse. */
