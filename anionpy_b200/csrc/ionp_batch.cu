@@ -79,9 +79,12 @@ struct BatchCall {
     int64_t w, rs;       // reduce: extent and stride of the reduced axis
     int64_t ostride;     // reduce: input distance between consecutive outer indices
     int64_t inner;       // col: kept inner extent
-    FastDiv idiv;        // col: division by inner
+    int64_t cols;        // col: inner outputs per tile
+    int64_t ninner;      // col: tiles across the inner extent
+    int32_t stage;       // col: elements per shared-memory stage
+    int32_t pad0;
     uint64_t seed;
-    void* partial;       // split: two partials per output
+    void* partial;       // split: `split` partials per output
     uint32_t* arrive;    // split: arrival counter per output
     uint32_t* flags;     // FPE word of the call
 };
@@ -203,18 +206,20 @@ __device__ __forceinline__ void bin_dispatch(const BatchCall& c, int64_t local) 
 }
 
 // --------------------------------------------------------------- reduction
-// Split combine: the tile that arrives second folds (left, right) in order.
+// Split combine: each part parks its partial; the tile that arrives last
+// folds the `split` partials left to right (part 0 first), then finishes.
 template <class P, int CD>
 __device__ __forceinline__ void split_combine(const BatchCall& c, int64_t o, int h, typename P::A part, bool is_final_value) {
     typedef typename P::A A;
-    A* pp = reinterpret_cast<A*>(c.partial);
-    pp[2 * o + h] = part;
+    const int np = c.split;
+    A* pp = reinterpret_cast<A*>(c.partial) + o * np;
+    pp[h] = part;
     __threadfence();
     const unsigned prev = atomicAdd(&c.arrive[o], 1u);
-    if (prev == 1u) {
+    if (prev == (unsigned)(np - 1)) {
         __threadfence();
-        const A left = *(volatile A*)&pp[2 * o], right = *(volatile A*)&pp[2 * o + 1];
-        const A tot = P::fold(left, right);
+        A tot = *(volatile A*)&pp[0];
+        for (int k = 1; k < np; ++k) tot = P::fold(tot, *(volatile A*)&pp[k]);
         if (is_final_value) store_cast<CD>(c.o, o, c.dto, (typename P::T)tot);
         else store_cast<CD>(c.o, o, c.dto, P::finish(tot, c.has_seed, c.seed));
     }
@@ -261,49 +266,71 @@ __device__ __noinline__ void row_tile(const BatchCall& c, int64_t local, unsigne
     }
 }
 
+// Column tile: one outer index, `cols` adjacent inner outputs, one part of
+// the reduced extent. The whole CTA streams stages of (rows x cols) elements
+// (coalesced along the inner axis) through shared memory, loading the next
+// stage into registers while the owner threads fold the current one in row
+// order, so a few long sequential folds still keep many loads in flight.
 template <int OP, int CD, bool CASTLD>
-__device__ __noinline__ void col_tile(const BatchCall& c, int64_t local) {
+__device__ __noinline__ void col_tile(const BatchCall& c, int64_t local, unsigned char* smem) {
     typedef typename DT<CD>::T T;
-    const int split = c.split;
-    const int64_t chunk = split == 2 ? local >> 1 : local;
-    const int h = split == 2 ? (int)(local & 1) : 0;
-    const int64_t half = c.w / 2;
-    const int64_t j0 = split == 2 && h ? half : 0;
-    const int64_t j1 = split == 2 && !h ? half : c.w;
-    const int64_t o0 = chunk * c.per_tile;
-    // raw compute-dtype loads (integer widening on load): the sequential
-    // folds run in the compute dtype itself, float16 included
+    constexpr int PER = 8;  // elements each thread loads per stage
     auto ld = [&](int64_t e) -> T {
         if constexpr (CASTLD) return load_int_widen<CD>(c.a, e, c.dta);
         else return reinterpret_cast<const T*>(c.a)[e];
     };
-    for (int64_t k = threadIdx.x; k < c.per_tile; k += BT_THREADS) {
-        const int64_t o = o0 + k;
-        if (o >= c.n) break;
-        const uint32_t outer = fdiv((uint32_t)o, c.idiv);
-        const int64_t in_ = o - (int64_t)outer * c.inner;
-        const int64_t base = (int64_t)outer * c.ostride + in_;
-        T acc;
-        bool have = false;
-        if (h == 0 && c.has_seed) { memcpy(&acc, &c.seed, sizeof(T)); have = true; }
-        int64_t j = j0;
-        for (; j + 8 <= j1; j += 8) {
-            T x[8];
+    const int np = c.split;
+    const int64_t chunk = local / np;
+    const int h = (int)(local - chunk * np);
+    const int64_t outer = chunk / c.ninner;
+    const int64_t i0 = (chunk - outer * c.ninner) * c.cols;
+    const int cn = (int)(c.inner - i0 < c.cols ? c.inner - i0 : c.cols);
+    const int64_t j0 = c.w * h / np, j1 = c.w * (h + 1) / np;
+    const int64_t base = outer * c.ostride + i0;
+    const int rows = c.stage / cn > 0 ? c.stage / cn : 1;
+    T* buf = reinterpret_cast<T*>(smem);
+    const int tid = threadIdx.x;
+    const bool owner = tid < cn;
+    T acc;
+    bool have = false;
+    if (owner && h == 0 && c.has_seed) { memcpy(&acc, &c.seed, sizeof(T)); have = true; }
+    T v[PER];
+    auto load_stage = [&](int64_t js) {
+        const int nr = (int)(j1 - js < rows ? j1 - js : rows);
+        const int tot = nr * cn;
 #pragma unroll
-            for (int u = 0; u < 8; ++u) x[u] = ld(base + (j + u) * c.rs);
-#pragma unroll
-            for (int u = 0; u < 8; ++u) {
-                if (!have) { acc = x[u]; have = true; }
-                else acc = BinOp<OP, CD>::apply(acc, x[u]);
+        for (int k = 0; k < PER; ++k) {
+            const int q = tid + k * BT_THREADS;
+            if (q < tot) {
+                const int r = q / cn, col = q - r * cn;
+                v[k] = ld(base + (js + r) * c.inner + col);
             }
         }
-        for (; j < j1; ++j) {
-            T x = ld(base + j * c.rs);
-            if (!have) { acc = x; have = true; }
-            else acc = BinOp<OP, CD>::apply(acc, x);
+    };
+    if (j0 < j1) load_stage(j0);
+    for (int64_t js = j0; js < j1; js += rows) {
+        const int nr = (int)(j1 - js < rows ? j1 - js : rows);
+        const int tot = nr * cn;
+#pragma unroll
+        for (int k = 0; k < PER; ++k) {
+            const int q = tid + k * BT_THREADS;
+            if (q < tot) buf[q] = v[k];
         }
-        if (split == 2) {
-            typedef RPol<OP, CD> PF;  // accumulator = compute dtype for the sequential folds
+        __syncthreads();
+        if (js + rows < j1) load_stage(js + rows);  // next stage in flight during the fold
+        if (owner) {
+            for (int r = 0; r < nr; ++r) {
+                const T x = buf[r * cn + tid];
+                if (!have) { acc = x; have = true; }
+                else acc = BinOp<OP, CD>::apply(acc, x);
+            }
+        }
+        __syncthreads();
+    }
+    if (owner) {
+        const int64_t o = outer * c.inner + i0 + tid;
+        if (np > 1) {
+            typedef RPol<OP, CD> PF;  // the accumulator is the compute dtype for these folds
             if constexpr (std::is_same<typename PF::A, T>::value) split_combine<PF, CD>(c, o, h, acc, true);
         } else {
             store_cast<CD>(c.o, o, c.dto, acc);
@@ -313,7 +340,7 @@ __device__ __noinline__ void col_tile(const BatchCall& c, int64_t local) {
 
 template <int OP, int CD, bool CASTLD>
 __device__ __forceinline__ void red_tile(const BatchCall& c, int64_t local, unsigned char* smem) {
-    if (c.kind == BK_COL) { col_tile<OP, CD, CASTLD>(c, local); return; }
+    if (c.kind == BK_COL) { col_tile<OP, CD, CASTLD>(c, local, smem); return; }
     switch (c.tpr) {
         case 1: row_tile<OP, CD, CASTLD, 1>(c, local, smem); break;
         case 32: row_tile<OP, CD, CASTLD, 32>(c, local, smem); break;
@@ -482,7 +509,9 @@ void tile_call(BatchCall& c, const IonpSchedule& s) {
     const bool assoc = red_assoc(c.op, c.cd);
     if (c.kind == BK_ROW) {
         c.tpr = c.w <= PW_BLOCK ? 1 : c.w <= 2048 ? 32 : BT_THREADS;
-        c.split = (s.red_split == 2 && c.tpr == BT_THREADS) ? 2 : 1;
+        // runs longer than 2^18 always split at the root: the slot tree of
+        // a half then fits 36 KB of shared memory (four CTAs per SM)
+        c.split = ((s.red_split == 2 || c.w > ((int64_t)1 << 18)) && c.tpr == BT_THREADS) ? 2 : 1;
         if (c.split == 2) {
             const int64_t n2 = pw_split(c.w);
             c.D = std::max(tree_depth(n2), tree_depth(c.w - n2));
@@ -496,14 +525,24 @@ void tile_call(BatchCall& c, const IonpSchedule& s) {
         }
         return;
     }
-    // column: the split halves the reduced extent, exact only for the
-    // associative folds
-    c.split = (s.red_split == 2 && assoc && c.w >= 2) ? 2 : 1;
-    c.per_tile = (int64_t)s.block_tile * s.elems_per_thread;
-    c.ntiles = ceil_div(c.n, c.per_tile) * c.split;
+    // column: `cols` adjacent inner outputs per tile (the block tile, at
+    // most one per thread); stages of 1024 x elems_per_thread/2 (at least
+    // 1024, at most 2048) elements; red_split = 2 cuts the reduced extent
+    // into parts of >= 4096 rows (up to 32), exact only for the associative
+    // folds
+    c.cols = std::min<int64_t>(c.inner, std::min(s.block_tile, BT_THREADS));
+    c.ninner = ceil_div(c.inner, c.cols);
+    c.stage = s.elems_per_thread == 4 ? 2048 : 1024;
+    c.per_tile = c.cols;
+    int np = 1;
+    if (s.red_split == 2 && assoc) np = (int)std::min<int64_t>(32, std::max<int64_t>(2, c.w / 4096));
+    if (np > c.w) np = (int)std::max<int64_t>(c.w, 1);
+    c.split = np;
+    c.ntiles = (c.n / c.inner) * c.ninner * np;
 }
 
 size_t row_smem(const BatchCall& c) {
+    if (c.kind == BK_COL) return (size_t)c.stage * dt_size(c.cd);
     if (c.kind != BK_ROW || c.tpr < 32) return 0;
     size_t acc = (c.cd == DT_F16 && c.op == OP_ADD) ? 4 : (size_t)dt_size(c.cd);
     size_t groups = BT_THREADS / c.tpr;
@@ -513,7 +552,7 @@ size_t row_smem(const BatchCall& c) {
 int64_t tile_cost(const BatchCall& c) {
     if (c.kind == BK_BINARY) return c.per_tile * (dt_size(c.dta) + dt_size(c.dtb) + dt_size(c.dto));
     if (c.kind == BK_ROW) return (c.split == 2 ? c.w / 2 : c.per_tile * c.w) * dt_size(c.dta);
-    return c.per_tile * (c.split == 2 ? c.w / 2 : c.w) * dt_size(c.dta);
+    return c.cols * (c.w / c.split) * dt_size(c.dta);
 }
 
 void set_default_schedule(IonpSchedule* s) {
@@ -542,8 +581,8 @@ int32_t upload_and_plan(IonpBatch* b, cudaStream_t s) {
         qq[k] = q[order[k]];
         qq[k].tile0 = tiles;
         tiles += qq[k].ntiles;
-        if (qq[k].kind != BK_BINARY && qq[k].split == 2) {
-            part += (size_t)qq[k].n * 16;
+        if (qq[k].kind != BK_BINARY && qq[k].split > 1) {
+            part += (size_t)qq[k].n * qq[k].split * 8;
             arr += (size_t)qq[k].n * 4;
         }
     }
@@ -569,10 +608,10 @@ int32_t upload_and_plan(IonpBatch* b, cudaStream_t s) {
     for (int k = 0; k < nc; ++k) {
         BatchCall& c = qq[k];
         c.flags = b->d_flags + c.user_id;
-        if (c.kind != BK_BINARY && c.split == 2) {
+        if (c.kind != BK_BINARY && c.split > 1) {
             c.partial = (char*)b->d_partial + po;
             c.arrive = (uint32_t*)((char*)b->d_arrive + ao);
-            po += (size_t)c.n * 16;
+            po += (size_t)c.n * c.split * 8;
             ao += (size_t)c.n * 4;
         }
     }
@@ -760,7 +799,6 @@ int32_t ionp_batch_add_reduce(IonpBatch* b, int32_t op, const IonpArr* a, int32_
         c.rs = inner;
         c.inner = inner;
         c.ostride = ext * inner;
-        c.idiv = make_div((uint32_t)inner);
     }
     c.user_id = (int32_t)b->calls.size();
     IonpSchedule s;
@@ -888,11 +926,11 @@ int32_t ionp_batch_time_call(IonpBatch* b, int32_t call, int32_t nsched, const I
             if ((st = cuda_err(cudaMemsetAsync(b->d_one_map, 0, sizeof(int32_t) * b->one_cap, s), "time map"))) break;
         }
         void* part = nullptr;
-        if (c.kind != BK_BINARY && c.split == 2) {
-            part = scratch_alloc((size_t)c.n * 20, s);
+        if (c.kind != BK_BINARY && c.split > 1) {
+            part = scratch_alloc((size_t)c.n * (c.split * 8 + 4), s);
             if (!part) { st = IONP_ERR_OOM; break; }
             c.partial = part;
-            c.arrive = (uint32_t*)((char*)part + (size_t)c.n * 16);
+            c.arrive = (uint32_t*)((char*)part + (size_t)c.n * c.split * 8);
         }
         const size_t smem = row_smem(c);
         if (smem > 48 * 1024 &&
