@@ -101,6 +101,17 @@ _SIGS = {
     "ionp_batch_run_per_call": [ctypes.c_void_p, ctypes.c_void_p],
     "ionp_batch_fpe": [ctypes.c_void_p, ctypes.POINTER(ctypes.c_uint32), ctypes.c_void_p],
     "ionp_batch_info": [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int64)],
+    "ionp_batch_features": [ctypes.c_void_p, ctypes.c_int32, ctypes.POINTER(ctypes.c_float)],
+    "ionp_mlp_create": [ctypes.POINTER(ctypes.c_void_p), ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_uint64],
+    "ionp_mlp_destroy": [ctypes.c_void_p],
+    "ionp_mlp_num_params": [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int64)],
+    "ionp_mlp_get": [ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p, ctypes.c_int64],
+    "ionp_mlp_set_params": [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64],
+    "ionp_mlp_forward": [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p, ctypes.c_void_p],
+    "ionp_mlp_gradients": [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32,
+                           ctypes.POINTER(ctypes.c_float), ctypes.c_void_p],
+    "ionp_mlp_train_step": [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32,
+                            ctypes.c_float, ctypes.c_float, ctypes.POINTER(ctypes.c_float), ctypes.c_void_p],
     "ionp_batch_time_call": [ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32, _S, ctypes.c_int32,
                              ctypes.POINTER(ctypes.c_float), ctypes.c_void_p],
     "ionp_device_info": [ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_int32), ctypes.c_char_p, ctypes.c_size_t],

@@ -894,6 +894,60 @@ int32_t ionp_batch_info(IonpBatch* b, int64_t* info) {
     return IONP_OK;
 }
 
+// Feature vector of one call for the schedule picker (IONP_PICKER_FEATURES
+// floats): op class, call kind, operand and result widths, merged shape,
+// stride class, reduction geometry.
+int32_t ionp_batch_features(IonpBatch* b, int32_t call, float* f) {
+    if (!b || !f || call < 0 || call >= (int32_t)b->calls.size()) return set_err(IONP_ERR_INVALID, "bad arguments");
+    const BatchCall& c = b->calls[call];
+    for (int i = 0; i < IONP_PICKER_FEATURES; ++i) f[i] = 0.0f;
+    auto lg = [](double v) { return (float)(std::log2(std::max(v, 1.0)) / 20.0); };
+    auto lb = [](int dt) { return (float)(std::log2((double)dt_size(dt)) / 3.0); };
+    int opc = 0;
+    if (c.kind == BK_BINARY) {
+        switch (c.op) {
+            case OP_ADD: opc = 0; break; case OP_SUBTRACT: opc = 1; break; case OP_MULTIPLY: opc = 2; break;
+            case OP_MAXIMUM: opc = 3; break; case OP_LESS: opc = 4; break; default: opc = 5; break;
+        }
+    } else {
+        opc = c.op == OP_ADD ? 6 : 7;
+    }
+    f[opc] = 1.0f;
+    f[8 + c.kind] = 1.0f;
+    f[11] = lb(c.dta);
+    f[12] = c.kind == BK_BINARY ? lb(c.dtb) : lb(c.dta);
+    f[13] = lb(c.dto);
+    f[14] = (c.dta == c.cd && (c.kind != BK_BINARY || c.dtb == c.cd)) ? 1.0f : 0.0f;
+    f[20] = lg((double)c.n);
+    int sclass = 0;  // 0 contiguous, 1 broadcast, 2 permuted, 3 strided
+    if (c.kind == BK_BINARY) {
+        f[15] = c.nd / 4.0f;
+        for (int i = 0; i < c.nd; ++i) f[16 + i] = lg((double)c.shape[c.nd - 1 - i]);
+        bool zero = false;
+        for (int i = 0; i < c.nd; ++i) zero = zero || c.sa[i] == 0 || c.sb[i] == 0;
+        const int64_t ia = std::llabs(c.sa[c.nd - 1]), ib = std::llabs(c.sb[c.nd - 1]), io = std::llabs(c.so[c.nd - 1]);
+        if (zero) sclass = 1;
+        else if (ia == 1 && ib == 1 && io == 1) sclass = 0;
+        else if (io == 1 && (ia > 1 || ib > 1)) sclass = 2;
+        else sclass = 3;
+    } else {
+        f[15] = 0.25f;
+        f[16] = lg((double)(c.n / std::max<int64_t>(c.kind == BK_COL ? c.inner : 1, 1)));
+        f[17] = lg((double)c.w);
+        f[18] = lg((double)(c.kind == BK_COL ? c.inner : 1));
+        sclass = c.kind == BK_ROW ? 0 : 3;
+    }
+    f[21 + sclass] = 1.0f;
+    f[25] = c.vec ? 1.0f : 0.0f;
+    f[26] = lg((double)(c.kind == BK_BINARY ? 1 : c.w));
+    f[27] = dt_is_float(c.cd) ? 1.0f : 0.0f;
+    f[28] = c.cd == DT_F16 ? 1.0f : 0.0f;
+    f[29] = (c.kind != BK_BINARY && c.dta != c.cd) ? 1.0f : 0.0f;
+    f[30] = lb(c.cd);
+    f[31] = 1.0f;
+    return IONP_OK;
+}
+
 // Device time of one call of the batch under each of the given schedules:
 // the call alone is run `reps` times back to back as its own queue, between
 // two events, after one untimed run.

@@ -33,7 +33,7 @@ class CallSpec:
     shapes: list                   # operand shapes
     dtypes: list                   # operand dtype names
     axis: int = 0                  # reduce only
-    ref: object = field(default=None, repr=False)
+    layouts: list = field(default_factory=list)  # per operand: "c", "T" (axes reversed), "s2" (step-2 inner axis)
 
 
 def _shape(rng, n, rank):
@@ -73,6 +73,25 @@ def mixed_stream(ncalls=10000, seed=7, n_min=10, n_max=10 ** 6):
     return calls, skipped
 
 
+def picker_cases(ncases, seed, n_min=10, n_max=10 ** 6):
+    """Cases of the schedule-picker study: drawn like the mixed stream, with
+    binary operands also laid out as axis-reversed views (permuted) or step-2
+    slices of the innermost axis (strided), 15% each, so that every stride
+    class appears (contiguous / broadcast / permuted / strided)."""
+    calls, _ = mixed_stream(ncases, seed=seed, n_min=n_min, n_max=n_max)
+    rng = np.random.default_rng(seed + 1000)
+    for c in calls:
+        if c.kind == "binary":
+            lay = []
+            for _ in range(2):
+                u = rng.random()
+                lay.append("T" if u < 0.15 else ("s2" if u < 0.30 else "c"))
+            c.layouts = lay
+        else:
+            c.layouts = ["c"]
+    return calls
+
+
 def pool_values(dt, n, rng):
     dt = np.dtype(dt)
     if dt == np.bool_:
@@ -100,6 +119,22 @@ class DevicePools:
             self.host[d] = h
             self.dev[d] = ap.from_numpy(h)
 
+    def view(self, shape, dt, layout="c"):
+        """A device array of the given logical shape laid out as `layout`
+        ("c": C-contiguous, "T": the transpose of a C-contiguous array of the
+        reversed shape, "s2": every other element of a C-contiguous array
+        twice as long in the innermost axis); also its host copy."""
+        shape = list(shape)
+        if layout == "T" and len(shape) > 1:
+            base, hb = self.array(shape[::-1], dt)
+            return base.transpose(), hb.transpose()
+        if layout == "s2" and len(shape) >= 1:
+            wide = shape[:-1] + [2 * shape[-1]]
+            base, hb = self.array(wide, dt)
+            idx = (slice(None),) * (len(shape) - 1) + (slice(None, None, 2),)
+            return base[idx], hb[idx]
+        return self.array(shape, dt)
+
     def array(self, shape, dt):
         """A new C-contiguous device array of random values; also returns its
         host copy (a view of the pool)."""
@@ -125,8 +160,9 @@ def build_batch(ap, calls, pools, keep_host=False):
     for c in calls:
         if c.kind == "binary":
             (sa, sb), (da, db) = c.shapes, c.dtypes
-            x, hx = pools.array(sa, da)
-            y, hy = pools.array(sb, db)
+            la, lb = c.layouts if c.layouts else ("c", "c")
+            x, hx = pools.view(sa, da, la)
+            y, hy = pools.view(sb, db, lb)
             b.add_binary(c.op, x, y)
             hosts.append((hx, hy) if keep_host else None)
         else:

@@ -321,6 +321,17 @@ def mixed_stream_bench(ap, L, steps, warmup, ncalls=10000, check_every=10, sched
            "calls_per_s_persistent_graph": round(len(calls) / (t_graph / 1e3)),
            "speedup_graph_vs_per_launch": round(t_per / t_graph, 2),
            "GB/s_persistent_graph": round(b.info()["bytes"] / (t_graph / 1e3) / 1e9, 1)}
+    if schedules == "learned":
+        from anionpy_b200 import picker
+        import time as _time
+        if os.path.exists(picker.DEFAULT_WEIGHTS):
+            t0 = _time.perf_counter()
+            sp = picker.SchedulePicker()
+            schedules = sp.pick(b)
+            res["picker"] = {"pick_s": round(_time.perf_counter() - t0, 3), "fallback_calls": sp.fallbacks,
+                             "distinct_schedules": int(len(set(schedules.tolist())))}
+        else:
+            schedules = None
     if schedules is not None:
         b.set_schedules(schedules)
         t_learn = timed(lambda: b.run(graph=True))
@@ -597,7 +608,7 @@ def main():
 
     mixed = None
     if rank == 0 and not args.no_stream:
-        mixed, _ = mixed_stream_bench(ap, L, args.steps, args.warmup)
+        mixed, _ = mixed_stream_bench(ap, L, args.steps, args.warmup, schedules="learned")
 
     # end-to-end through the public API with pinned host buffers
     e2e = None

@@ -222,6 +222,32 @@ int32_t ionp_batch_info(IonpBatch* b, int64_t* info);
 int32_t ionp_batch_time_call(IonpBatch* b, int32_t call, int32_t nsched, const IonpSchedule* scheds, int32_t reps,
                              float* us_out, IonpStream stream);
 
+/* Feature vector of one queued call for the schedule picker. */
+#define IONP_PICKER_FEATURES 32
+int32_t ionp_batch_features(IonpBatch* b, int32_t call, float* features);
+
+/* ------------------------------------------------------- schedule picker net */
+/* A 3-layer perceptron (FP32, ReLU hidden layers) with hand-written forward,
+ * backward and Adam kernels; it predicts each schedule's log-time from a
+ * call's features. No counterpart in the reference. x, t, mask and y are
+ * DEVICE float arrays, row-major [batch][features] / [batch][outputs]. */
+typedef struct IonpMlp IonpMlp;
+int32_t ionp_mlp_create(IonpMlp** m, int32_t nin, int32_t hidden, int32_t nout, uint64_t seed);
+int32_t ionp_mlp_destroy(IonpMlp* m);
+int32_t ionp_mlp_num_params(IonpMlp* m, int64_t* n);
+/* which = 0: parameters; 1: gradients of the last gradients/train step.
+ * Layout: W1[nin][h], b1[h], W2[h][h], b2[h], W3[h][nout], b3[nout]. */
+int32_t ionp_mlp_get(IonpMlp* m, int32_t which, float* host, int64_t n);
+int32_t ionp_mlp_set_params(IonpMlp* m, const float* host, int64_t n);
+int32_t ionp_mlp_forward(IonpMlp* m, const float* x, int32_t batch, float* y, IonpStream stream);
+/* mean squared error over the (masked) outputs and its gradients; loss may be
+ * NULL (then the call does not wait for the stream) */
+int32_t ionp_mlp_gradients(IonpMlp* m, const float* x, const float* t, const float* mask, int32_t batch, float* loss,
+                           IonpStream stream);
+/* gradients + one Adam step (beta 0.9 / 0.999, eps 1e-8, decoupled-free L2 weight_decay) */
+int32_t ionp_mlp_train_step(IonpMlp* m, const float* x, const float* t, const float* mask, int32_t batch, float lr,
+                            float weight_decay, float* loss, IonpStream stream);
+
 /* ---------------------------------------------------------------- memory */
 /* Caching device allocator (the device counterpart of Buffer's Vec<T>,
  * ionp-core/src/buffer.rs:18): size-classed free lists, stream-ordered reuse. */
