@@ -6,7 +6,13 @@ precision (no library tables are copied):
   the constant to ~160 bits (each part is the round-to-nearest remainder);
 * TWO_OVER_PI[]: the binary expansion of 2/pi in 32-bit words (bit 1 of the
   fraction is the MSB of word 0), enough for Payne-Hanek reduction of every
-  finite double.
+  finite double;
+* EXP2_64_TAB[]: 2^(j/64), j = 0..63, as double-double pairs (hi, lo), and
+  LN2_64_1/2/3: ln(2)/64 in three parts, for the table-driven float64 exp;
+* LOG_INV_TAB[] / LOG_TAB[]: for y in [1 + j/128, 1 + (j+1)/128), a 9-bit
+  reciprocal inv_j of the interval midpoint (inv_0 = 1 exactly) and
+  -log(inv_j) as a double-double pair, for the table-driven float64 log
+  (y * inv_j - 1 is exact with one fused multiply-add).
 
 Run: python anionpy_b200/csrc/gen_constants.py > anionpy_b200/csrc/ionp_constants.h
 """
@@ -47,6 +53,33 @@ def main():
     print("    constexpr uint32_t W[48] = {" + ", ".join(f"0x{w:08X}u" for w in words) + "};")
     print("    return (i >= 0 && i < 48) ? W[i] : 0u;")
     print("}")
+    ln2_64 = split3(mpmath.log(2) / 64)
+    for i, p in enumerate(ln2_64):
+        print(f"constexpr double LN2_64_{i + 1} = {p.hex()};")
+    print("// 2^(j/64): hi, lo")
+    tab = []
+    for j in range(64):
+        v = mpmath.power(2, mpmath.mpf(j) / 64)
+        hi = float(v)
+        lo = float(v - mpmath.mpf(hi))
+        tab += [hi, lo]
+    print("__device__ static const double EXP2_64_TAB[128] = {" + ", ".join(t.hex() for t in tab) + "};")
+    invs, logs = [], []
+    for j in range(128):
+        if j == 0:
+            k = 512
+        else:
+            mid = 1 + (mpmath.mpf(j) + mpmath.mpf(0.5)) / 128
+            k = int(mpmath.nint(512 / mid))
+        inv = mpmath.mpf(k) / 512
+        invs.append(float(inv))
+        lv = -mpmath.log(inv)
+        hi = float(lv)
+        lo = float(lv - mpmath.mpf(hi))
+        logs += [hi, lo]
+    print("// 9-bit reciprocals of the log table intervals, and -log of each (hi, lo)")
+    print("__device__ static const double LOG_INV_TAB[128] = {" + ", ".join(t.hex() for t in invs) + "};")
+    print("__device__ static const double LOG_TAB[256] = {" + ", ".join(t.hex() for t in logs) + "};")
     print("}  // namespace ionp")
 
 

@@ -59,18 +59,146 @@ __device__ __forceinline__ float cr_sinf(float x) {
     return sinf_slow(x);
 }
 
+// ---------------------------------------------------------------------------
+// float64 exp / log: a table-driven first pass accurate to about 2^-67
+// (relative for exp, absolute for log), then Ziv's rounding test: if the
+// first-pass value y_hi + y_lo, moved by its error bound either way, rounds to
+// the same double, that double is the correctly rounded result; otherwise
+// (about one argument in 2^11) the double-double evaluation decides. Every
+// product that must be exact is a fused multiply-add (__fma_rn); everything
+// else rounds as written (the library is built with -fmad=false).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void quick_two_sum(double a, double b, double* s, double* e) {  // |a| >= |b|
+    *s = a + b;
+    *e = b - (*s - a);
+}
+__device__ __forceinline__ void full_two_sum(double a, double b, double* s, double* e) {
+    *s = a + b;
+    const double bb = *s - a;
+    *e = (a - (*s - bb)) + (b - bb);
+}
+
+// Tang's method with 64 table entries: x = k ln2/64 + r, |r| <= ln2/128,
+// e^x = 2^(k >> 6) * 2^((k & 63)/64) * (1 + r + q), q = r^2/2 + ... + r^7/5040
+// (the next term is below 2^-75). Error of y_hi + y_lo below 2^-66 relative.
+__device__ __forceinline__ double exp_first(double x, bool* ok) {
+    constexpr double INV = 1.0 / LN2_64_1;
+    const double k = rint(x * INV);
+    const int ki = (int)k;
+    const int j = ki & 63, m = ki >> 6;
+    const double p1 = k * LN2_64_1;
+    const double p1e = __fma_rn(k, LN2_64_1, -p1);   // exact product error
+    const double s = x - p1;                          // exact (Sterbenz)
+    const double t = __fma_rn(k, LN2_64_2, p1e);
+    double rh, rl;
+    full_two_sum(s, -t, &rh, &rl);
+    rl = rl - k * LN2_64_3;
+    double q = __fma_rn(rh, 1.0 / 5040.0, 1.0 / 720.0);
+    q = __fma_rn(q, rh, 1.0 / 120.0);
+    q = __fma_rn(q, rh, 1.0 / 24.0);
+    q = __fma_rn(q, rh, 1.0 / 6.0);
+    q = __fma_rn(q, rh, 0.5);
+    q = q * (rh * rh);
+    const double tr = __fma_rn(rh, rl, rl) + q;      // e^(rh+rl) - 1 - rh
+    const double th = __ldg(&EXP2_64_TAB[2 * j]), tl = __ldg(&EXP2_64_TAB[2 * j + 1]);
+    const double ph = th * rh;
+    const double pl = __fma_rn(th, rh, -ph);
+    double sh, sl;
+    quick_two_sum(th, ph, &sh, &sl);
+    const double tail = __fma_rn(th, tr, __fma_rn(tl, rh, tl) + (pl + sl));
+    double yh, yl;
+    quick_two_sum(sh, tail, &yh, &yl);
+    const double eb = yh * 0x1p-66;
+    const double a = yh + (yl + eb), b = yh + (yl - eb);
+    *ok = a == b;
+    // 2^m, m in [-1021, 1022] on the first-pass range
+    return a * __longlong_as_double((long long)(1023 + m) << 52);
+}
+
+// log x = e ln2 - log(inv_j) + log1p(r), r = y inv_j - 1 exact (y = the
+// mantissa in [1, 2), inv_j a 9-bit reciprocal, |r| <= 2^-7.6), log1p(r) =
+// r + q, q to r^9/9. Near 1 (|x - 1| < 2^-7) log1p(x - 1) directly, with
+// r^2/2 split exactly. Absolute error of y_hi + y_lo below 2^-66 (table
+// path) or |r| 2^-66 (near 1).
+__device__ __forceinline__ double log_first(double x, bool* ok) {
+    double yh, yl, eb;
+    const double d1 = x - 1.0;
+    if (fabs(d1) < 0x1p-7) {
+        const double r = d1;                          // exact (Sterbenz)
+        const double hh = r * r;
+        const double hl = __fma_rn(r, r, -hh);
+        double q = __fma_rn(r, -1.0 / 10.0, 1.0 / 9.0);
+        q = __fma_rn(q, r, -1.0 / 8.0);
+        q = __fma_rn(q, r, 1.0 / 7.0);
+        q = __fma_rn(q, r, -1.0 / 6.0);
+        q = __fma_rn(q, r, 1.0 / 5.0);
+        q = __fma_rn(q, r, -1.0 / 4.0);
+        q = __fma_rn(q, r, 1.0 / 3.0);
+        q = q * (hh * r);                             // r^3/3 - ... + r^10/10 (sign per term)
+        double s, se;
+        quick_two_sum(r, -0.5 * hh, &s, &se);
+        const double tail = se + (q - 0.5 * hl);
+        quick_two_sum(s, tail, &yh, &yl);
+        eb = fabs(r) * 0x1p-66;
+    } else {
+        uint64_t bits = (uint64_t)__double_as_longlong(x);
+        int e = 0;
+        if (bits < (1ull << 52)) {                   // subnormal: scale into the normal range
+            bits = (uint64_t)__double_as_longlong(x * 0x1p54);
+            e = -54;
+        }
+        e += (int)(bits >> 52) - 1023;
+        const double y = __longlong_as_double((long long)((bits & 0xFFFFFFFFFFFFFull) | 0x3FF0000000000000ull));
+        const int j = (int)((bits >> 45) & 127);
+        const double inv = __ldg(&LOG_INV_TAB[j]);
+        const double lh = __ldg(&LOG_TAB[2 * j]), ll = __ldg(&LOG_TAB[2 * j + 1]);
+        const double r = __fma_rn(y, inv, -1.0);     // exact
+        double q = __fma_rn(r, 1.0 / 9.0, -1.0 / 8.0);
+        q = __fma_rn(q, r, 1.0 / 7.0);
+        q = __fma_rn(q, r, -1.0 / 6.0);
+        q = __fma_rn(q, r, 1.0 / 5.0);
+        q = __fma_rn(q, r, -1.0 / 4.0);
+        q = __fma_rn(q, r, 1.0 / 3.0);
+        q = __fma_rn(q, r, -0.5);
+        q = q * (r * r);                              // log1p(r) - r
+        const double E = (double)e;
+        const double ah = E * LN2_1;
+        const double al = __fma_rn(E, LN2_1, -ah) + E * LN2_2;
+        double s1, e1, s2, e2;
+        full_two_sum(ah, lh, &s1, &e1);
+        full_two_sum(s1, r, &s2, &e2);
+        const double tail = ((e1 + e2) + (al + ll)) + q;
+        quick_two_sum(s2, tail, &yh, &yl);
+        eb = 0x1p-66 + fabs(yh) * 0x1p-90;
+    }
+    const double a = yh + (yl + eb), b = yh + (yl - eb);
+    *ok = a == b;
+    return a;
+}
+
+static __device__ __noinline__ double exp_slow(double x) { return dd::exp_dd(x).hi; }
+static __device__ __noinline__ double log_slow(double x) { return dd::log_dd(x).hi; }
+
 __device__ __forceinline__ double cr_exp(double x) {
     if (isnan_d(x)) return quiet_d(x);
     if (x > 709.8) return __longlong_as_double(0x7FF0000000000000ll);
     if (x < -745.2) return 0.0;
-    return dd::exp_dd(x).hi;
+    if (x >= -708.0 && x <= 709.0) {  // normal results: the table-driven pass
+        bool ok;
+        const double r = exp_first(x, &ok);
+        if (ok) return r;
+    }
+    return exp_slow(x);
 }
 __device__ __forceinline__ double cr_log(double x) {
     if (isnan_d(x)) return quiet_d(x);
     if (x < 0.0) return dnan_d();
     if (x == 0.0) return __longlong_as_double((long long)0xFFF0000000000000ull);
     if (isinf(x)) return x;
-    return dd::log_dd(x).hi;
+    bool ok;
+    const double r = log_first(x, &ok);
+    if (ok) return r;
+    return log_slow(x);
 }
 __device__ __forceinline__ double cr_sin(double x) {
     if (isnan_d(x)) return quiet_d(x);

@@ -88,6 +88,32 @@ def test_float64_correctly_rounded(fn):
     assert got[nan].tobytes() == ref[nan].tobytes(), "NaN payloads"
 
 
+def stress64(fn, n, seed):
+    """float64 arguments at the edges of the table-driven first pass: near
+    the table's interval ends, around |x - 1| = 2^-7 for log, subnormals,
+    powers of two, the ends of exp's normal range, tiny arguments."""
+    rng = np.random.default_rng(seed)
+    if fn == "exp":
+        k = rng.integers(-65000, 65000, n // 2)
+        parts = [k * (np.log(2) / 64) + rng.uniform(-1e-9, 1e-9, n // 2),
+                 rng.uniform(-708.5, -707.5, n // 8), rng.uniform(708.5, 709.9, n // 8),
+                 rng.uniform(-1e-12, 1e-12, n // 8) * np.exp2(-rng.integers(0, 40, n // 8))]
+    else:
+        parts = [1 + rng.uniform(-2 ** -6, 2 ** -6, n // 2), 1 + rng.uniform(-1e-12, 1e-12, n // 8),
+                 np.exp2(rng.integers(-1074, 1024, n // 8).astype(np.float64)),
+                 rng.uniform(0, 1, n // 8) * 2.0 ** -1030, 1 + np.arange(1, 129) / 128.0]
+    return np.concatenate(parts).astype(np.float64)
+
+
+@pytest.mark.parametrize("fn", ["exp", "log"])
+def test_float64_first_pass_edges(fn):
+    x = stress64(fn, 24000, 5)
+    got = getattr(ap, fn)(ap.from_numpy(x)).get()
+    want = cr_f64(fn, x)
+    ok = np.isfinite(want)
+    assert_bits_equal(got[ok], want[ok], f"{fn} float64 edges vs correctly rounded")
+
+
 @pytest.mark.parametrize("fn", ["exp", "log", "sin"])
 def test_float16_and_int_promotion(fn):
     rng = np.random.default_rng(3)
