@@ -12,7 +12,9 @@ precision (no library tables are copied):
 * LOG_INV_TAB[] / LOG_TAB[]: for y in [1 + j/128, 1 + (j+1)/128), a 9-bit
   reciprocal inv_j of the interval midpoint (inv_0 = 1 exactly) and
   -log(inv_j) as a double-double pair, for the table-driven float64 log
-  (y * inv_j - 1 is exact with one fused multiply-add).
+  (y * inv_j - 1 is exact with one fused multiply-add);
+* SINCOS_64_TAB[]: sin(i/64) and cos(i/64), i = 0..51, as double-double
+  pairs (sin hi, sin lo, cos hi, cos lo), for the table-driven float64 sin.
 
 Run: python anionpy_b200/csrc/gen_constants.py > anionpy_b200/csrc/ionp_constants.h
 """
@@ -80,6 +82,14 @@ def main():
     print("// 9-bit reciprocals of the log table intervals, and -log of each (hi, lo)")
     print("__device__ static const double LOG_INV_TAB[128] = {" + ", ".join(t.hex() for t in invs) + "};")
     print("__device__ static const double LOG_TAB[256] = {" + ", ".join(t.hex() for t in logs) + "};")
+    sc = []
+    for i in range(52):
+        a = mpmath.mpf(i) / 64
+        for v in (mpmath.sin(a), mpmath.cos(a)):
+            hi = float(v)
+            sc += [hi, float(v - mpmath.mpf(hi))]
+    print("// sin(i/64) hi, lo, cos(i/64) hi, lo")
+    print("__device__ static const double SINCOS_64_TAB[208] = {" + ", ".join(t.hex() for t in sc) + "};")
     print("}  // namespace ionp")
 
 

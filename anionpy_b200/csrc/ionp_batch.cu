@@ -82,7 +82,8 @@ struct BatchCall {
     int64_t cols;        // col: inner outputs per tile
     int64_t ninner;      // col: tiles across the inner extent
     int32_t stage;       // col: elements per shared-memory stage
-    int32_t pad0;
+    int32_t copies;      // times the call is queued (the autotuner's throughput runs; else 1)
+    int64_t ntiles_one;  // tiles of one copy
     uint64_t seed;
     void* partial;       // split: `split` partials per output
     uint32_t* arrive;    // split: arrival counter per output
@@ -209,13 +210,15 @@ __device__ __forceinline__ void bin_dispatch(const BatchCall& c, int64_t local) 
 // Split combine: each part parks its partial; the tile that arrives last
 // folds the `split` partials left to right (part 0 first), then finishes.
 template <class P, int CD>
-__device__ __forceinline__ void split_combine(const BatchCall& c, int64_t o, int h, typename P::A part, bool is_final_value) {
+__device__ __forceinline__ void split_combine(const BatchCall& c, int64_t o, int64_t rep, int h, typename P::A part,
+                                              bool is_final_value) {
     typedef typename P::A A;
     const int np = c.split;
-    A* pp = reinterpret_cast<A*>(c.partial) + o * np;
+    const int64_t slot = rep * c.n + o;  // each queued copy has its own partials
+    A* pp = reinterpret_cast<A*>(c.partial) + slot * np;
     pp[h] = part;
     __threadfence();
-    const unsigned prev = atomicAdd(&c.arrive[o], 1u);
+    const unsigned prev = atomicAdd(&c.arrive[slot], 1u);
     if (prev == (unsigned)(np - 1)) {
         __threadfence();
         A tot = *(volatile A*)&pp[0];
@@ -226,7 +229,7 @@ __device__ __forceinline__ void split_combine(const BatchCall& c, int64_t o, int
 }
 
 template <int OP, int CD, bool CASTLD, int TPR>
-__device__ __noinline__ void row_tile(const BatchCall& c, int64_t local, unsigned char* smem) {
+__device__ __noinline__ void row_tile(const BatchCall& c, int64_t local, int64_t rep, unsigned char* smem) {
     typedef RPol<OP, CD, CASTLD> P;
     typedef typename P::A A;
     constexpr int G = BT_THREADS / TPR;
@@ -243,7 +246,7 @@ __device__ __noinline__ void row_tile(const BatchCall& c, int64_t local, unsigne
             const int64_t n2 = pw_split(c.w);
             const int64_t soff = h ? n2 : 0, slen = h ? c.w - n2 : n2;
             A r = group_tree_t<P, TPR>(c.a, c.dta, c.rs, o * c.ostride, soff, slen, c.D, slots, valid, t);
-            if (t == 0) split_combine<P, CD>(c, o, h, r, false);
+            if (t == 0) split_combine<P, CD>(c, o, rep, h, r, false);
         }
         return;
     }
@@ -272,7 +275,7 @@ __device__ __noinline__ void row_tile(const BatchCall& c, int64_t local, unsigne
 // stage into registers while the owner threads fold the current one in row
 // order, so a few long sequential folds still keep many loads in flight.
 template <int OP, int CD, bool CASTLD>
-__device__ __noinline__ void col_tile(const BatchCall& c, int64_t local, unsigned char* smem) {
+__device__ __noinline__ void col_tile(const BatchCall& c, int64_t local, int64_t rep, unsigned char* smem) {
     typedef typename DT<CD>::T T;
     constexpr int PER = 8;  // elements each thread loads per stage
     auto ld = [&](int64_t e) -> T {
@@ -331,7 +334,7 @@ __device__ __noinline__ void col_tile(const BatchCall& c, int64_t local, unsigne
         const int64_t o = outer * c.inner + i0 + tid;
         if (np > 1) {
             typedef RPol<OP, CD> PF;  // the accumulator is the compute dtype for these folds
-            if constexpr (std::is_same<typename PF::A, T>::value) split_combine<PF, CD>(c, o, h, acc, true);
+            if constexpr (std::is_same<typename PF::A, T>::value) split_combine<PF, CD>(c, o, rep, h, acc, true);
         } else {
             store_cast<CD>(c.o, o, c.dto, acc);
         }
@@ -339,72 +342,107 @@ __device__ __noinline__ void col_tile(const BatchCall& c, int64_t local, unsigne
 }
 
 template <int OP, int CD, bool CASTLD>
-__device__ __forceinline__ void red_tile(const BatchCall& c, int64_t local, unsigned char* smem) {
-    if (c.kind == BK_COL) { col_tile<OP, CD, CASTLD>(c, local, smem); return; }
+__device__ __forceinline__ void red_tile(const BatchCall& c, int64_t local, int64_t rep, unsigned char* smem) {
+    if (c.kind == BK_COL) { col_tile<OP, CD, CASTLD>(c, local, rep, smem); return; }
     switch (c.tpr) {
-        case 1: row_tile<OP, CD, CASTLD, 1>(c, local, smem); break;
-        case 32: row_tile<OP, CD, CASTLD, 32>(c, local, smem); break;
-        default: row_tile<OP, CD, CASTLD, BT_THREADS>(c, local, smem); break;
+        case 1: row_tile<OP, CD, CASTLD, 1>(c, local, rep, smem); break;
+        case 32: row_tile<OP, CD, CASTLD, 32>(c, local, rep, smem); break;
+        default: row_tile<OP, CD, CASTLD, BT_THREADS>(c, local, rep, smem); break;
     }
 }
 
-__device__ __forceinline__ void red_dispatch(const BatchCall& c, int64_t local, unsigned char* smem) {
+__device__ __forceinline__ void red_dispatch(const BatchCall& c, int64_t local, int64_t rep, unsigned char* smem) {
     if (c.op == OP_ADD) {
         switch (c.cd) {
-            case DT_I64: red_tile<OP_ADD, DT_I64, true>(c, local, smem); break;
-            case DT_U64: red_tile<OP_ADD, DT_U64, true>(c, local, smem); break;
-            case DT_F16: red_tile<OP_ADD, DT_F16, false>(c, local, smem); break;
-            case DT_F32: red_tile<OP_ADD, DT_F32, false>(c, local, smem); break;
-            case DT_F64: red_tile<OP_ADD, DT_F64, false>(c, local, smem); break;
+            case DT_I64: red_tile<OP_ADD, DT_I64, true>(c, local, rep, smem); break;
+            case DT_U64: red_tile<OP_ADD, DT_U64, true>(c, local, rep, smem); break;
+            case DT_F16: red_tile<OP_ADD, DT_F16, false>(c, local, rep, smem); break;
+            case DT_F32: red_tile<OP_ADD, DT_F32, false>(c, local, rep, smem); break;
+            case DT_F64: red_tile<OP_ADD, DT_F64, false>(c, local, rep, smem); break;
         }
         return;
     }
 #define IONP_MCASE(D) \
-    case D: red_tile<OP_MAXIMUM, D, false>(c, local, smem); break;
+    case D: red_tile<OP_MAXIMUM, D, false>(c, local, rep, smem); break;
     switch (c.cd) { IONP_DTS(IONP_MCASE) }
 #undef IONP_MCASE
 }
 
 // The persistent kernel: claim tiles until the queue is drained.
+__device__ __forceinline__ void cp_async4(void* smem, const void* gmem) {
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+
+__device__ __forceinline__ void run_tile(const BatchCall& c, int64_t t, unsigned char* smem) {
+    int64_t local = t - c.tile0;
+    const int64_t rep = local / c.ntiles_one;  // the copy (0 outside autotuner runs)
+    local -= rep * c.ntiles_one;
+    if (c.kind == BK_BINARY) {
+        switch (c.op) {
+            case OP_ADD: bin_dispatch<OP_ADD>(c, local); break;
+            case OP_SUBTRACT: bin_dispatch<OP_SUBTRACT>(c, local); break;
+            case OP_MULTIPLY: bin_dispatch<OP_MULTIPLY>(c, local); break;
+            case OP_MAXIMUM: bin_dispatch<OP_MAXIMUM>(c, local); break;
+            case OP_LESS: bin_dispatch<OP_LESS>(c, local); break;
+            case OP_LOGICAL_AND: bin_dispatch<OP_LOGICAL_AND>(c, local); break;
+        }
+    } else {
+        red_dispatch(c, local, rep, smem);
+    }
+}
+
+// The persistent kernel: claim tiles until the queue is drained. The next
+// tile is claimed, and its descriptor (when it belongs to another call)
+// copied into the second shared-memory slot with cp.async, while the
+// current tile runs, so neither the claim nor the descriptor load sits on
+// the critical path.
 __global__ void __launch_bounds__(BT_THREADS) k_batch(const BatchCall* __restrict__ calls,
                                                       const int32_t* __restrict__ tile_call, int64_t ntiles,
                                                       unsigned long long* next) {
     extern __shared__ __align__(16) unsigned char smem[];
-    __shared__ BatchCall sc;
+    __shared__ BatchCall sc[2];
     __shared__ int64_t s_tile;
     __shared__ int32_t s_call;
-    int cur = -1;
-    for (;;) {
+    constexpr int WORDS = (int)(sizeof(BatchCall) / 4);
+    if (threadIdx.x == 0) {
+        const int64_t t0 = (int64_t)atomicAdd(next, 1ull);
+        s_tile = t0;
+        s_call = t0 < ntiles ? tile_call[t0] : -1;
+    }
+    __syncthreads();
+    int64_t t = s_tile;
+    int have0 = s_call, have1 = -1;  // descriptor held by slot 0 / 1 (uniform)
+    int use = 0;
+    if (t < ntiles) {
+        const uint32_t* src = reinterpret_cast<const uint32_t*>(calls + have0);
+        uint32_t* dst = reinterpret_cast<uint32_t*>(&sc[0]);
+        for (int i = threadIdx.x; i < WORDS; i += BT_THREADS) dst[i] = src[i];
+    }
+    __syncthreads();
+    while (t < ntiles) {
         if (threadIdx.x == 0) {
-            const int64_t t = (int64_t)atomicAdd(next, 1ull);
-            s_tile = t;
-            s_call = t < ntiles ? tile_call[t] : -1;
+            const int64_t t2 = (int64_t)atomicAdd(next, 1ull);
+            s_tile = t2;
+            s_call = t2 < ntiles ? tile_call[t2] : -1;
         }
         __syncthreads();
-        const int64_t t = s_tile;
-        const int ci = s_call;
-        if (t >= ntiles) break;
-        if (ci != cur) {
-            const uint32_t* src = reinterpret_cast<const uint32_t*>(calls + ci);
-            uint32_t* dst = reinterpret_cast<uint32_t*>(&sc);
-            for (int i = threadIdx.x; i < (int)(sizeof(BatchCall) / 4); i += BT_THREADS) dst[i] = src[i];
-            cur = ci;
-            __syncthreads();
+        const int64_t t2 = s_tile;
+        const int c2 = s_call;
+        const int cur = use ? have1 : have0;
+        const int oth = use ? have0 : have1;
+        if (c2 >= 0 && c2 != cur && c2 != oth) {
+            const uint32_t* src = reinterpret_cast<const uint32_t*>(calls + c2);
+            uint32_t* dst = reinterpret_cast<uint32_t*>(&sc[use ^ 1]);
+            for (int i = threadIdx.x; i < WORDS; i += BT_THREADS) cp_async4(dst + i, src + i);
+            if (use) have0 = c2; else have1 = c2;
         }
-        const int64_t local = t - sc.tile0;
-        if (sc.kind == BK_BINARY) {
-            switch (sc.op) {
-                case OP_ADD: bin_dispatch<OP_ADD>(sc, local); break;
-                case OP_SUBTRACT: bin_dispatch<OP_SUBTRACT>(sc, local); break;
-                case OP_MULTIPLY: bin_dispatch<OP_MULTIPLY>(sc, local); break;
-                case OP_MAXIMUM: bin_dispatch<OP_MAXIMUM>(sc, local); break;
-                case OP_LESS: bin_dispatch<OP_LESS>(sc, local); break;
-                case OP_LOGICAL_AND: bin_dispatch<OP_LOGICAL_AND>(sc, local); break;
-            }
-        } else {
-            red_dispatch(sc, local, smem);
-        }
+        asm volatile("cp.async.commit_group;\n" ::: "memory");
+        run_tile(sc[use], t, smem);
+        asm volatile("cp.async.wait_group 0;\n" ::: "memory");
         __syncthreads();
+        t = t2;
+        if (c2 >= 0 && c2 != cur) use ^= 1;
     }
 }
 
@@ -492,9 +530,18 @@ int32_t check_schedule(const IonpSchedule* s) {
     return ok ? IONP_OK : set_err(IONP_ERR_INVALID, "schedule outside the 48-point space");
 }
 
+void tile_geometry(BatchCall& c, const IonpSchedule& s);
+
 // Tile geometry of one call under its schedule (fills per_tile, ntiles,
-// split and D; everything else was planned when the call was added).
+// split and D; everything else was planned when the call was added). One
+// copy of the call.
 void tile_call(BatchCall& c, const IonpSchedule& s) {
+    tile_geometry(c, s);
+    c.copies = 1;
+    c.ntiles_one = c.ntiles;
+}
+
+void tile_geometry(BatchCall& c, const IonpSchedule& s) {
     c.bt = s.block_tile;
     c.vw = s.vec_width;
     c.ept = s.elems_per_thread;
@@ -948,9 +995,12 @@ int32_t ionp_batch_features(IonpBatch* b, int32_t call, float* f) {
     return IONP_OK;
 }
 
-// Device time of one call of the batch under each of the given schedules:
-// the call alone is run `reps` times back to back as its own queue, between
-// two events, after one untimed run.
+// Device time of one call of the batch under each of the given schedules,
+// as the batch sees it: with the GPU saturated. The call is queued `copies`
+// times in one persistent launch (enough copies for four tiles per resident
+// CTA, at most 4096; copies of a big call: one), the launch is run `reps`
+// times back to back between two events after one untimed run, and the time
+// per copy is reported. Copies write identical values to the same output.
 int32_t ionp_batch_time_call(IonpBatch* b, int32_t call, int32_t nsched, const IonpSchedule* scheds, int32_t reps,
                              float* us_out, IonpStream stream) {
     int32_t st = IONP_OK;
@@ -958,8 +1008,11 @@ int32_t ionp_batch_time_call(IonpBatch* b, int32_t call, int32_t nsched, const I
         return set_err(IONP_ERR_INVALID, "bad arguments");
     cudaStream_t s = (cudaStream_t)stream;
     if (!b->finalized && (st = upload_and_plan(b, s))) return st;
+    // the call's descriptor four times, the tile map cycling through them:
+    // like a mixed queue, consecutive claims of a CTA switch descriptors
+    constexpr int NDESC = 4;
     if (!b->d_one) {
-        b->d_one = (BatchCall*)scratch_alloc(sizeof(BatchCall), s);
+        b->d_one = (BatchCall*)scratch_alloc(sizeof(BatchCall) * NDESC, s);
         if (!b->d_one) return IONP_ERR_OOM;
     }
     cudaEvent_t e0, e1;
@@ -971,32 +1024,43 @@ int32_t ionp_batch_time_call(IonpBatch* b, int32_t call, int32_t nsched, const I
         tile_call(c, scheds[k]);
         c.tile0 = 0;
         c.flags = b->d_flags + c.user_id;
-        // tile -> call map of a one-call queue: all zeros
-        if (c.ntiles > b->one_cap) {
-            if (b->d_one_map) scratch_free(b->d_one_map, s);
-            b->one_cap = std::max<int64_t>(c.ntiles, 4096);
-            b->d_one_map = (int32_t*)scratch_alloc(sizeof(int32_t) * b->one_cap, s);
-            if (!b->d_one_map) { b->one_cap = 0; st = IONP_ERR_OOM; break; }
-            if ((st = cuda_err(cudaMemsetAsync(b->d_one_map, 0, sizeof(int32_t) * b->one_cap, s), "time map"))) break;
-        }
-        void* part = nullptr;
-        if (c.kind != BK_BINARY && c.split > 1) {
-            part = scratch_alloc((size_t)c.n * (c.split * 8 + 4), s);
-            if (!part) { st = IONP_ERR_OOM; break; }
-            c.partial = part;
-            c.arrive = (uint32_t*)((char*)part + (size_t)c.n * c.split * 8);
-        }
         const size_t smem = row_smem(c);
         if (smem > 48 * 1024 &&
             (st = cuda_err(cudaFuncSetAttribute(k_batch, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem), "time smem")))
             break;
         int per_sm = 1;
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch, BT_THREADS, smem);
-        const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(c.ntiles, (int64_t)std::max(per_sm, 1) * b->sms));
-        if ((st = cuda_err(cudaMemcpyAsync(b->d_one, &c, sizeof(BatchCall), cudaMemcpyHostToDevice, s), "time upload"))) break;
+        const int64_t slots = (int64_t)std::max(per_sm, 1) * b->sms;
+        if (c.ntiles_one > 0) {
+            c.copies = (int32_t)std::min<int64_t>(4096, std::max<int64_t>(1, ceil_div(4 * slots, c.ntiles_one)));
+            c.ntiles = c.ntiles_one * c.copies;
+        }
+        if (c.ntiles > b->one_cap) {
+            if (b->d_one_map) scratch_free(b->d_one_map, s);
+            b->one_cap = std::max<int64_t>(c.ntiles, 4096);
+            b->d_one_map = (int32_t*)scratch_alloc(sizeof(int32_t) * b->one_cap, s);
+            if (!b->d_one_map) { b->one_cap = 0; st = IONP_ERR_OOM; break; }
+            std::vector<int32_t> cyc((size_t)b->one_cap);
+            for (size_t i = 0; i < cyc.size(); ++i) cyc[i] = (int32_t)(i % NDESC);
+            if ((st = cuda_err(cudaMemcpy(b->d_one_map, cyc.data(), sizeof(int32_t) * cyc.size(), cudaMemcpyHostToDevice),
+                               "time map")))
+                break;
+        }
+        void* part = nullptr;
+        const size_t nslot = (size_t)c.n * c.copies;
+        if (c.kind != BK_BINARY && c.split > 1) {
+            part = scratch_alloc(nslot * (c.split * 8 + 4), s);
+            if (!part) { st = IONP_ERR_OOM; break; }
+            c.partial = part;
+            c.arrive = (uint32_t*)((char*)part + nslot * c.split * 8);
+        }
+        const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(c.ntiles, slots));
+        BatchCall descs[NDESC];
+        for (int q = 0; q < NDESC; ++q) descs[q] = c;
+        if ((st = cuda_err(cudaMemcpyAsync(b->d_one, descs, sizeof(descs), cudaMemcpyHostToDevice, s), "time upload"))) break;
         auto one = [&]() {
             cudaMemsetAsync(b->d_next, 0, 8, s);
-            if (c.arrive) cudaMemsetAsync(c.arrive, 0, (size_t)c.n * 4, s);
+            if (c.arrive) cudaMemsetAsync(c.arrive, 0, nslot * 4, s);
             if (c.ntiles) k_batch<<<grid, BT_THREADS, smem, s>>>(b->d_one, b->d_one_map, c.ntiles, b->d_next);
             count_launch();
         };
@@ -1011,7 +1075,7 @@ int32_t ionp_batch_time_call(IonpBatch* b, int32_t call, int32_t nsched, const I
         if (st) break;
         float ms = 0;
         cudaEventElapsedTime(&ms, e0, e1);
-        us_out[k] = ms * 1000.0f / reps;
+        us_out[k] = ms * 1000.0f / ((float)reps * (float)c.copies);
         if ((st = cuda_err(cudaGetLastError(), "time launch"))) break;
     }
     cudaEventDestroy(e0);

@@ -160,6 +160,66 @@ k_bin_nd(EwDesc d, uint32_t* flags) {
     if constexpr (FPE) flush_flags(bits, flags);
 }
 
+// Two merged dims whose operands disagree on which dim is contiguous (a
+// transposed view against a C-ordered one): 32 x 32 tiles staged through
+// shared memory. Each operand is read along its own contiguous dim, the
+// output written along its own, so every global access is coalesced.
+constexpr int TR_TILE = 32;
+template <class T> __device__ __forceinline__ void tr_load(T (*sm)[TR_TILE + 1], const T* p, int64_t s0, int64_t s1,
+                                                         int64_t i0, int64_t j0, int64_t R, int64_t C) {
+    const int tid = threadIdx.x;
+    if (s0 == 1 && s1 != 1) {  // column-contiguous: consecutive threads walk rows
+#pragma unroll
+        for (int k = 0; k < TR_TILE * TR_TILE / EW_THREADS; ++k) {
+            const int r = tid % TR_TILE, c = tid / TR_TILE + k * (EW_THREADS / TR_TILE);
+            if (i0 + r < R && j0 + c < C) sm[r][c] = p[(i0 + r) * s0 + (j0 + c) * s1];
+        }
+    } else {                   // row-contiguous (or broadcast): consecutive threads walk columns
+#pragma unroll
+        for (int k = 0; k < TR_TILE * TR_TILE / EW_THREADS; ++k) {
+            const int c = tid % TR_TILE, r = tid / TR_TILE + k * (EW_THREADS / TR_TILE);
+            if (i0 + r < R && j0 + c < C) sm[r][c] = p[(i0 + r) * s0 + (j0 + c) * s1];
+        }
+    }
+}
+
+template <int OP, int CD, bool FPE>
+__global__ void __launch_bounds__(EW_THREADS)
+k_bin_tr(EwDesc d, uint32_t* flags) {
+    typedef typename DT<CD>::T T;
+    typedef BinOp<OP, CD> Op;
+    typedef typename Op::R R;
+    __shared__ T sa[TR_TILE][TR_TILE + 1], sb[TR_TILE][TR_TILE + 1];
+    uint32_t bits = 0;
+    const int64_t R0 = d.shape[0], C0 = d.shape[1];
+    const int64_t tr = (R0 + TR_TILE - 1) / TR_TILE, tc = (C0 + TR_TILE - 1) / TR_TILE;
+    const T* pa = (const T*)d.a.p;
+    const T* pb = (const T*)d.b.p;
+    R* po = (R*)d.o;
+    const bool ocol = d.so[0] == 1 && d.so[1] != 1;
+    const int tid = threadIdx.x;
+    for (int64_t t = blockIdx.x; t < tr * tc; t += gridDim.x) {
+        const int64_t i0 = (t / tc) * TR_TILE, j0 = (t % tc) * TR_TILE;
+        tr_load<T>(sa, pa, d.a.st[0], d.a.st[1], i0, j0, R0, C0);
+        tr_load<T>(sb, pb, d.b.st[0], d.b.st[1], i0, j0, R0, C0);
+        __syncthreads();
+#pragma unroll
+        for (int k = 0; k < TR_TILE * TR_TILE / EW_THREADS; ++k) {
+            int r, c;
+            if (ocol) { r = tid % TR_TILE; c = tid / TR_TILE + k * (EW_THREADS / TR_TILE); }
+            else { c = tid % TR_TILE; r = tid / TR_TILE + k * (EW_THREADS / TR_TILE); }
+            if (i0 + r < R0 && j0 + c < C0) {
+                const T x = sa[r][c], y = sb[r][c];
+                const R v = Op::apply(x, y);
+                if constexpr (FPE) bits |= fpe_bits<OP, CD>(x, y, v);
+                po[(i0 + r) * d.so[0] + (j0 + c) * d.so[1]] = v;
+            }
+        }
+        __syncthreads();
+    }
+    if constexpr (FPE) flush_flags(bits, flags);
+}
+
 // ---------------------------------------------------------------------------
 // unary
 // ---------------------------------------------------------------------------

@@ -40,6 +40,22 @@ cudaError_t launch_bin_t(const EwDesc& d, const ContigInfo& ci, uint32_t* flags,
         return cudaGetLastError();
     }
     const bool same = d.a.dt == CD && d.b.dt == CD && d.odt == BinOp<OP, CD>::OUT_DT && d.m.p == nullptr;
+    // two merged dims with operands contiguous along different dims: tiles
+    // through shared memory
+    if (same && d.nd == 2 && d.shape[0] >= TR_TILE && d.shape[1] >= TR_TILE) {
+        auto colc = [](int64_t s0, int64_t s1) { return s0 == 1 && s1 != 1; };
+        const bool ca = colc(d.a.st[0], d.a.st[1]), cb = colc(d.b.st[0], d.b.st[1]), co = colc(d.so[0], d.so[1]);
+        if (ca != co || cb != co) {
+            const int64_t tiles = ((d.shape[0] + TR_TILE - 1) / TR_TILE) * ((d.shape[1] + TR_TILE - 1) / TR_TILE);
+            const int g = (int)(tiles < 148 * 8 ? tiles : 148 * 8);
+            if constexpr (HAS_FPE) {
+                if (fpe) { k_bin_tr<OP, CD, true><<<g, EW_THREADS, 0, s>>>(d, flags); count_launch(); return cudaGetLastError(); }
+            }
+            k_bin_tr<OP, CD, false><<<g, EW_THREADS, 0, s>>>(d, flags);
+            count_launch();
+            return cudaGetLastError();
+        }
+    }
     int64_t inner = d.shape[d.nd - 1];
     int g = ew_grid(inner >= 64 ? (d.n + 3) / 4 : d.n);
     if constexpr (HAS_FPE) {

@@ -878,15 +878,35 @@ __global__ void __launch_bounds__(RED_THREADS) k_argext(RedDesc d) {
         if (!live) hi = lo;
         T best{};
         int64_t bi = -1;
-        for (int64_t i = lo + t; i < hi; i += TPR) {
-            int64_t off = 0, rem = i;
-            for (int k = d.nr - 1; k >= 0; --k) {
-                int64_t id = rem % d.rshape[k];
-                rem /= d.rshape[k];
-                off += id * d.rst[k];
+        if (d.nr == 1) {
+            // one strided run: no index arithmetic per element, eight loads
+            // in flight per thread, each thread's elements in increasing order
+            const T* p = (const T*)d.a + base;
+            const int64_t ws = d.rst[0];
+            int64_t i = lo + t;
+            for (; i + 7 * TPR < hi; i += 8 * TPR) {
+                T x[8];
+#pragma unroll
+                for (int u = 0; u < 8; ++u) x[u] = p[(i + (int64_t)u * TPR) * ws];
+#pragma unroll
+                for (int u = 0; u < 8; ++u)
+                    if (bi < 0 || P::better(x[u], best)) { best = x[u]; bi = i + (int64_t)u * TPR; }
             }
-            T v = ((const T*)d.a)[base + off];
-            if (bi < 0 || P::better(v, best)) { best = v; bi = i; }
+            for (; i < hi; i += TPR) {
+                T v = p[i * ws];
+                if (bi < 0 || P::better(v, best)) { best = v; bi = i; }
+            }
+        } else {
+            for (int64_t i = lo + t; i < hi; i += TPR) {
+                int64_t off = 0, rem = i;
+                for (int k = d.nr - 1; k >= 0; --k) {
+                    int64_t id = rem % d.rshape[k];
+                    rem /= d.rshape[k];
+                    off += id * d.rst[k];
+                }
+                T v = ((const T*)d.a)[base + off];
+                if (bi < 0 || P::better(v, best)) { best = v; bi = i; }
+            }
         }
         // combine across the group, lower lanes (earlier indices) first
         if constexpr (TPR > 1) {
@@ -954,7 +974,7 @@ __global__ void __launch_bounds__(RED_THREADS) k_argext_col(RedDesc d) {
         T best = p[0];
         int64_t bi = 0;
         int64_t i = 1;
-        constexpr int U = 8;
+        constexpr int U = 16;
         for (; i + U <= d.w; i += U) {
             T x[U];
 #pragma unroll

@@ -103,16 +103,35 @@ __device__ __forceinline__ double x_sqrt(double x) { return isnan_d(x) ? quiet_d
 
 // glibc fmod semantics (what Rust's float `%` calls): NaN operands propagate,
 // fmod(inf, y) and fmod(x, 0) are the default NaN, fmod(x, inf) = x.
+// Quotients below 2^23 (2^52): q = trunc(fl(x / y)) is the exact truncated
+// quotient or one too large in magnitude (rounding is monotone and every
+// integer below 2^24 is representable), x - q y is exact in one fused
+// multiply-add (the true remainder is representable; the one-too-large case
+// is within a factor two of y, so Sterbenz applies), and adding y back with
+// x's sign repairs the one-too-large case exactly. Larger quotients take the
+// library's fmod.
 __device__ __forceinline__ float x_fmod(float x, float y) {
     if (isnan_f(x) || isnan_f(y)) return nan2(x, y);
     if (isinf(x) || y == 0.0f) return dnan_f();
     if (isinf(y)) return x;
+    const float q = truncf(__fdiv_rn(x, y));
+    if (fabsf(q) < 0x1p23f) {
+        float r = __fmaf_rn(-q, y, x);
+        if (r != 0.0f && signbit(r) != signbit(x)) r = __fadd_rn(r, copysignf(y, x));
+        return r == 0.0f ? copysignf(0.0f, x) : r;
+    }
     return fmodf(x, y);
 }
 __device__ __forceinline__ double x_fmod(double x, double y) {
     if (isnan_d(x) || isnan_d(y)) return nan2(x, y);
     if (isinf(x) || y == 0.0) return dnan_d();
     if (isinf(y)) return x;
+    const double q = trunc(__ddiv_rn(x, y));
+    if (fabs(q) < 0x1p52) {
+        double r = __fma_rn(-q, y, x);
+        if (r != 0.0 && signbit(r) != signbit(x)) r = __dadd_rn(r, copysign(y, x));
+        return r == 0.0 ? copysign(0.0, x) : r;
+    }
     return fmod(x, y);
 }
 

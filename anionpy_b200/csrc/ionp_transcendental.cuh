@@ -200,11 +200,77 @@ __device__ __forceinline__ double cr_log(double x) {
     if (ok) return r;
     return log_slow(x);
 }
+// sin x for |x| <= 2^20: Cody-Waite reduction x = k pi/2 + r with pi/2 in
+// three parts (r as a double-double, error below |k| 2^-104), then
+// |r| = a + b with a = i/64 from a table of sin(a), cos(a) as double-double
+// pairs and |b| <= 1/128:
+//   sin(a + b) = S + C b + [S (cos b - 1) + C (sin b - b)]
+//   cos(a + b) = C - S b + [C (cos b - 1) - S (sin b - b)]
+// with the products C b, S b split exactly and the bracketed tails (below
+// 2^-14 relative) in double. Error of y_hi + y_lo below 2^-66 absolute (and
+// below 2^-62 relative when a = 0), plus the reduction error.
+__device__ __forceinline__ double sin_first(double x, bool* ok) {
+    constexpr double TWO_OVER_PI = 0.63661977236758134308;
+    const double k = rint(x * TWO_OVER_PI);
+    const int q = ((int)k) & 3;
+    const double p1 = k * PI_2_1;
+    const double p1e = __fma_rn(k, PI_2_1, -p1);
+    const double s = x - p1;                          // exact (Sterbenz)
+    const double t = __fma_rn(k, PI_2_2, p1e);
+    double rh, rl;
+    full_two_sum(s, -t, &rh, &rl);
+    rl = rl - k * PI_2_3;
+    const bool neg = rh < 0.0;
+    if (neg) { rh = -rh; rl = -rl; }
+    const int i = (int)rint(rh * 64.0);
+    const double bh = rh - (double)i * 0.015625;      // exact
+    const double bl = rl;
+    const double b2 = bh * bh;
+    double sbt = __fma_rn(b2, -1.0 / 5040.0, 1.0 / 120.0);
+    sbt = __fma_rn(sbt, b2, -1.0 / 6.0);
+    sbt = sbt * (b2 * bh);                            // sin b - b
+    double cbm = __fma_rn(b2, 1.0 / 40320.0, -1.0 / 720.0);
+    cbm = __fma_rn(cbm, b2, 1.0 / 24.0);
+    cbm = __fma_rn(cbm, b2, -0.5);
+    cbm = cbm * b2;                                   // cos b - 1
+    const double sh = __ldg(&SINCOS_64_TAB[4 * i]), sl = __ldg(&SINCOS_64_TAB[4 * i + 1]);
+    const double ch = __ldg(&SINCOS_64_TAB[4 * i + 2]), cl = __ldg(&SINCOS_64_TAB[4 * i + 3]);
+    double s1, e1, tail;
+    if ((q & 1) == 0) {   // sin r
+        const double ph = ch * bh;
+        const double pl = __fma_rn(ch, bh, -ph);
+        full_two_sum(sh, ph, &s1, &e1);
+        tail = (e1 + pl) + ((ch * bl + cl * bh) + sl) + (sh * cbm + ch * sbt);
+    } else {              // cos r
+        const double ph = sh * bh;
+        const double pl = __fma_rn(sh, bh, -ph);
+        full_two_sum(ch, -ph, &s1, &e1);
+        tail = (e1 - pl) + (cl - (sh * bl + sl * bh)) + (ch * cbm - sh * sbt);
+    }
+    double yh, yl;
+    quick_two_sum(s1, tail, &yh, &yl);
+    const double eb = (i == 0 && (q & 1) == 0 ? fabs(yh) * 0x1p-62 : 0x1p-66) + fabs(k) * 0x1p-103 + 0x1p-104;
+    const double a = yh + (yl + eb), b = yh + (yl - eb);
+    *ok = a == b;
+    // sin x = sin r, cos r, -sin r, -cos r for q = 0..3; sin(-r) = -sin r
+    const bool flip = (q >= 2) != (neg && (q & 1) == 0);
+    return flip ? -a : a;
+}
+
+static __device__ __noinline__ double sin_slow(double x) { return dd::sin_dd(x).hi; }
+
 __device__ __forceinline__ double cr_sin(double x) {
     if (isnan_d(x)) return quiet_d(x);
     if (isinf(x)) return dnan_d();
     if (x == 0.0) return x;
-    return dd::sin_dd(x).hi;
+    const double ax = fabs(x);
+    if (ax < 0x1p-26) return x;  // sin x = x (1 - x^2/6 ...) rounds to x
+    if (ax <= 0x1p20) {
+        bool ok;
+        const double r = sin_first(x, &ok);
+        if (ok) return r;
+    }
+    return sin_slow(x);
 }
 
 }  // namespace ionp

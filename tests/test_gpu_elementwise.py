@@ -123,6 +123,27 @@ def test_binary_layouts_and_order_k(op, dt):
         assert list(got.elem_strides) == list(want_st), f"{op} {name}: strides {got.elem_strides} != {want_st}"
 
 
+@pytest.mark.parametrize("dt", [np.float32, np.float64, np.int8, np.float16, np.int64], ids=lambda d: np.dtype(d).name)
+@pytest.mark.parametrize("shape", [(45, 77), (33, 1000), (257, 40)])
+def test_transposed_against_c_order_tiles(dt, shape):
+    """A transposed view against a C-ordered operand (the shared-memory tile
+    path), ragged tile edges, both output layouts via out=."""
+    rng = np.random.default_rng(8)
+    base = array(dt, shape[::-1], rng)
+    w = array(dt, shape, rng)
+    v = base.T
+    for op in ("add", "maximum", "multiply"):
+        want = O.binary(op, v, w)[0]
+        db = ap.from_numpy(base)
+        got = getattr(ap, op)(db.T, ap.from_numpy(w))
+        assert_bits_equal(got.get(), want, f"{op} {shape}")
+        for order in ("C", "F"):
+            host_out = np.zeros(shape, want.dtype, order=order)
+            dout = ap.from_numpy(host_out)
+            getattr(ap, op)(db.T, ap.from_numpy(w), out=dout)
+            assert_bits_equal(dout.get(), want, f"{op} {shape} out={order}")
+
+
 @pytest.mark.parametrize("op", ["negative", "absolute", "invert", "logical_not", "sqrt"])
 @pytest.mark.parametrize("dt", ALL, ids=lambda d: np.dtype(d).name)
 def test_unary_exact(op, dt):

@@ -91,13 +91,20 @@ def test_float64_correctly_rounded(fn):
 def stress64(fn, n, seed):
     """float64 arguments at the edges of the table-driven first pass: near
     the table's interval ends, around |x - 1| = 2^-7 for log, subnormals,
-    powers of two, the ends of exp's normal range, tiny arguments."""
+    powers of two, the ends of exp's normal range, tiny arguments, sin near
+    multiples of pi/2 and around the reduction limit 2^20."""
     rng = np.random.default_rng(seed)
     if fn == "exp":
         k = rng.integers(-65000, 65000, n // 2)
         parts = [k * (np.log(2) / 64) + rng.uniform(-1e-9, 1e-9, n // 2),
                  rng.uniform(-708.5, -707.5, n // 8), rng.uniform(708.5, 709.9, n // 8),
                  rng.uniform(-1e-12, 1e-12, n // 8) * np.exp2(-rng.integers(0, 40, n // 8))]
+    elif fn == "sin":
+        k = rng.integers(-600000, 600000, n // 4)
+        parts = [k * (np.pi / 2) + rng.uniform(-1e-6, 1e-6, n // 4),
+                 rng.integers(0, 52, n // 4) / 64.0 + rng.uniform(-2 ** -7, 2 ** -7, n // 4),
+                 rng.uniform(-2 ** 21, 2 ** 21, n // 8), rng.uniform(-1e-7, 1e-7, n // 8),
+                 (1 - 2 * rng.integers(0, 2, n // 8)) * np.exp2(rng.uniform(-30, 20, n // 8))]
     else:
         parts = [1 + rng.uniform(-2 ** -6, 2 ** -6, n // 2), 1 + rng.uniform(-1e-12, 1e-12, n // 8),
                  np.exp2(rng.integers(-1074, 1024, n // 8).astype(np.float64)),
@@ -105,7 +112,7 @@ def stress64(fn, n, seed):
     return np.concatenate(parts).astype(np.float64)
 
 
-@pytest.mark.parametrize("fn", ["exp", "log"])
+@pytest.mark.parametrize("fn", ["exp", "log", "sin"])
 def test_float64_first_pass_edges(fn):
     x = stress64(fn, 24000, 5)
     got = getattr(ap, fn)(ap.from_numpy(x)).get()
