@@ -431,6 +431,62 @@ def cpu_sample_cases(n):
     return out
 
 
+def cpu_reduce_cases(scale):
+    """The reduction inputs with the leading extent divided by `scale`."""
+    out = []
+    for tag, host, keepdims, initial in reduce_inputs(scale):
+        for op in RED_OPS:
+            for axis in RED_AXES:
+                nb = host.nbytes
+                out.append((op, host, axis, keepdims, initial if op != "argmax" else None, nb))
+    return out
+
+
+def _split_axis(a, axis):
+    """The axis along which independent outputs can be split between threads."""
+    if axis is None or a.ndim == 1:
+        return None
+    ax = axis % a.ndim
+    return 0 if ax != 0 else 1
+
+
+def time_oracle_reduce(cases, threads):
+    """Oracle reductions; the outputs are split between threads along a kept
+    axis (each output's fold order is unchanged); all-axis reductions run on
+    one thread (one ordered fold)."""
+    from concurrent.futures import ThreadPoolExecutor
+    from oracle import oracle as O
+    O.lib()
+    total = 0
+    t0 = time.perf_counter()
+    with ThreadPoolExecutor(max_workers=threads) as ex:
+        for op, a, axis, keepdims, initial, nb in cases:
+            sa = _split_axis(a, axis)
+            def one(x):
+                if op == "argmax":
+                    return O.argext("argmax", x, axis=axis, keepdims=keepdims)
+                kw = {"keepdims": keepdims}
+                if initial is not None:
+                    kw["initial"] = initial
+                return O.reduce(op, x, axis=axis, **kw)
+            if sa is None:
+                ex.submit(one, a).result()
+            else:
+                n = a.shape[sa]
+                parts = [(i * n // threads, (i + 1) * n // threads) for i in range(threads)]
+                fs = []
+                for lo, hi in parts:
+                    if hi > lo:
+                        idx = [slice(None)] * a.ndim
+                        idx[sa] = slice(lo, hi)
+                        fs.append(ex.submit(one, a[tuple(idx)]))
+                for f in fs:
+                    f.result()
+            total += nb
+    dt = time.perf_counter() - t0
+    return total, dt
+
+
 def time_oracle(cases, threads):
     from concurrent.futures import ThreadPoolExecutor
     from oracle import oracle as O
@@ -452,26 +508,38 @@ def time_oracle(cases, threads):
     return total_bytes / dt / 1e9, dt
 
 
+def cpu_step(cases, rcases, threads):
+    """GB/s of one pass over the sampled element-wise and reduction cases."""
+    v, dt = time_oracle(cases, threads)
+    rb, rdt = time_oracle_reduce(rcases, threads)
+    eb = v * dt * 1e9
+    return (eb + rb) / (dt + rdt) / 1e9, dt + rdt
+
+
 def reference_arm(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
     threads = os.cpu_count() or 1
     n = 1 << 21
+    red_scale = 64
     cases = cpu_sample_cases(n)
+    rcases = cpu_reduce_cases(red_scale)
     for _ in range(args.warmup):
         time_oracle(cases[:2], threads)
     vals = []
     for _ in range(args.steps):
-        v, _ = time_oracle(cases, threads)
+        v, _ = cpu_step(cases, rcases, threads)
         vals.append(v)
     value = statistics.median(vals)
-    sample = f"{len(cases)} contiguous sweep cases x {n} elements (2^21 of 2^28) per step, split over {threads} threads"
+    sample = (f"{len(cases)} contiguous sweep cases x {n} elements (2^21 of 2^28) and the {len(rcases)} reductions "
+              f"on inputs with the leading extent / {red_scale}, per step, split over {threads} threads")
     line = {
         "metric": METRIC, "value": round(value, 3), "unit": "GB/s", "n_gpus": args.gpus, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "mixed(int32,int64,f32,f64)", "data": "synthetic",
-        "config": {"workload": "large element-wise sweep, contiguous cases (bounded CPU sample)", "elements": n},
+        "config": {"workload": "large element-wise sweep (contiguous cases) + reductions (bounded CPU sample)",
+                   "elements": n, "reduce_scale": red_scale},
         "impl": "reference",
         "cpu_baseline": {"value": round(value, 3), "unit": "GB/s", "cores": threads, "kind": "port", "sample": sample},
         "e2e": {"value": round(value, 3), "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -496,6 +564,7 @@ def main():
     ap_.add_argument("--reduce-scale", type=int, default=1, help="divide the reductions' leading extent (small runs)")
     ap_.add_argument("--no-parity", action="store_true", help="skip the oracle checks after the timed region")
     ap_.add_argument("--no-stream", action="store_true", help="skip the batched mixed stream")
+    ap_.add_argument("--stream-calls", type=int, default=10000, help="calls in the mixed stream")
     args = ap_.parse_args()
     if args.impl == "reference":
         return reference_arm(args)
@@ -608,7 +677,7 @@ def main():
 
     mixed = None
     if rank == 0 and not args.no_stream:
-        mixed, _ = mixed_stream_bench(ap, L, args.steps, args.warmup, schedules="learned")
+        mixed, _ = mixed_stream_bench(ap, L, args.steps, args.warmup, ncalls=args.stream_calls, schedules="learned")
 
     # end-to-end through the public API with pinned host buffers
     e2e = None
@@ -618,10 +687,11 @@ def main():
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         sample_n = 1 << 22
-        v, secs = time_oracle(cpu_sample_cases(sample_n), 1)
+        v, secs = cpu_step(cpu_sample_cases(sample_n), cpu_reduce_cases(32), 1)
         cpu = {"value": round(v, 3), "unit": "GB/s", "cores": 1, "kind": "port",
-               "sample": f"the {len(cpu_sample_cases(16))} contiguous sweep cases at {sample_n} elements each (2^22 of 2^28), "
-                         f"single thread, {secs:.1f} s of CPU work"}
+               "sample": f"the {len(cpu_sample_cases(16))} contiguous sweep cases at {sample_n} elements each (2^22 of 2^28) "
+                         f"and the 27 reductions on inputs with the leading extent / 32, single thread, "
+                         f"{secs:.1f} s of CPU work"}
 
     if rank == 0:
         line = {
