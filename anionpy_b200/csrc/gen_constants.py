@@ -12,7 +12,8 @@ precision (no library tables are copied):
 * LOG_INV_TAB[] / LOG_TAB[]: for y in [1 + j/128, 1 + (j+1)/128), a 9-bit
   reciprocal inv_j of the interval midpoint (inv_0 = 1 exactly) and
   -log(inv_j) as a double-double pair, for the table-driven float64 log
-  (y * inv_j - 1 is exact with one fused multiply-add);
+  (y * inv_j - 1 is exact as a double-double: one product split by a fused
+  multiply-add);
 * SINCOS_64_TAB[]: sin(i/64) and cos(i/64), i = 0..51, as double-double
   pairs (sin hi, sin lo, cos hi, cos lo), for the table-driven float64 sin.
 

@@ -500,6 +500,7 @@ struct IonpBatch {
     BatchCall* d_one = nullptr;
     int32_t* d_one_map = nullptr;
     int64_t one_cap = 0;
+    char* d_pool = nullptr;  // the autotuner's operand pool
 };
 
 namespace {
@@ -516,6 +517,8 @@ void release_device(IonpBatch* b) {
     if (b->d_arrive) scratch_free(b->d_arrive, s);
     if (b->d_one) scratch_free(b->d_one, s);
     if (b->d_one_map) scratch_free(b->d_one_map, s);
+    if (b->d_pool) scratch_free(b->d_pool, s);
+    b->d_pool = nullptr;
     b->d_calls = nullptr; b->d_tile_call = nullptr; b->d_next = nullptr; b->d_flags = nullptr;
     b->d_partial = nullptr; b->d_arrive = nullptr; b->d_one = nullptr; b->d_one_map = nullptr;
     b->one_cap = 0;
@@ -996,11 +999,58 @@ int32_t ionp_batch_features(IonpBatch* b, int32_t call, float* f) {
 }
 
 // Device time of one call of the batch under each of the given schedules,
-// as the batch sees it: with the GPU saturated. The call is queued `copies`
-// times in one persistent launch (enough copies for four tiles per resident
-// CTA, at most 4096; copies of a big call: one), the launch is run `reps`
-// times back to back between two events after one untimed run, and the time
-// per copy is reported. Copies write identical values to the same output.
+// as the batch sees it. The call is queued `copies` times in one persistent
+// launch -- enough copies for four tiles per resident CTA (at most 4096),
+// limited so that all copies fit a 1 GiB pool -- and every copy reads and
+// writes its OWN region of that pool, so the copies stream from HBM like the
+// distinct calls of a real batch instead of re-reading one L2-resident
+// input. Timing needs only the call's shapes, strides and dtypes; the pool's
+// contents are whatever it holds. The launch is run `reps` times back to
+// back between two events after one untimed run; time per copy is reported.
+}  // extern "C"
+
+namespace ionp {
+namespace {
+constexpr size_t TIME_POOL = (size_t)1 << 30;
+
+// memory extent [lo, hi] in elements of an operand over the merged dims
+void extent(const int64_t* st, const int32_t* shape, int nd, int64_t* lo, int64_t* hi) {
+    *lo = 0; *hi = 0;
+    for (int i = 0; i < nd; ++i) {
+        const int64_t e = (int64_t)(shape[i] - 1) * st[i];
+        if (e < 0) *lo += e; else *hi += e;
+    }
+}
+size_t round256(size_t b) { return (b + 255) & ~(size_t)255; }
+
+// copy r of the template: its own operand regions, tiles and partials
+__global__ void k_replicate(const BatchCall* __restrict__ tmpl, BatchCall* __restrict__ out, int K, char* pool,
+                            int64_t span_a, int64_t span_b, int64_t span_o, int64_t lo_a, int64_t lo_b, int64_t lo_o,
+                            char* part, int64_t part_stride, uint32_t* arrive, int64_t arrive_stride) {
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= K) return;
+    BatchCall c = *tmpl;
+    char* base = pool + (int64_t)r * (span_a + span_b + span_o);
+    c.a = base - lo_a;
+    c.b = base + span_a - lo_b;
+    c.o = base + span_a + span_b - lo_o;
+    c.tile0 = (int64_t)r * c.ntiles_one;
+    if (part) {
+        c.partial = part + (int64_t)r * part_stride;
+        c.arrive = arrive + (int64_t)r * arrive_stride;
+    }
+    out[r] = c;
+}
+// copy-major tile map: tile t belongs to copy t / ntiles_one
+__global__ void k_copy_map(int32_t* map, int64_t n, int64_t per) {
+    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x)
+        map[t] = (int32_t)(t / per);
+}
+}  // namespace
+}  // namespace ionp
+
+extern "C" {
+
 int32_t ionp_batch_time_call(IonpBatch* b, int32_t call, int32_t nsched, const IonpSchedule* scheds, int32_t reps,
                              float* us_out, IonpStream stream) {
     int32_t st = IONP_OK;
@@ -1008,21 +1058,39 @@ int32_t ionp_batch_time_call(IonpBatch* b, int32_t call, int32_t nsched, const I
         return set_err(IONP_ERR_INVALID, "bad arguments");
     cudaStream_t s = (cudaStream_t)stream;
     if (!b->finalized && (st = upload_and_plan(b, s))) return st;
-    // the call's descriptor four times, the tile map cycling through them:
-    // like a mixed queue, consecutive claims of a CTA switch descriptors
-    constexpr int NDESC = 4;
+    constexpr int KMAX = 4096;
     if (!b->d_one) {
-        b->d_one = (BatchCall*)scratch_alloc(sizeof(BatchCall) * NDESC, s);
+        b->d_one = (BatchCall*)scratch_alloc(sizeof(BatchCall) * (KMAX + 1), s);
         if (!b->d_one) return IONP_ERR_OOM;
     }
+    if (!b->d_pool) {
+        b->d_pool = (char*)scratch_alloc(TIME_POOL, s);
+        if (!b->d_pool) return IONP_ERR_OOM;
+    }
+    // operand extents (bytes) of one copy, each 256-byte aligned
+    const BatchCall& c0 = b->calls[call];
+    int64_t lo_a = 0, lo_b = 0, lo_o = 0, hi_a = 0, hi_b = 0, hi_o = 0;
+    if (c0.kind == BK_BINARY) {
+        extent(c0.sa, c0.shape, c0.nd, &lo_a, &hi_a);
+        extent(c0.sb, c0.shape, c0.nd, &lo_b, &hi_b);
+        extent(c0.so, c0.shape, c0.nd, &lo_o, &hi_o);
+    } else {
+        hi_a = c0.n * c0.w - 1;
+        hi_o = c0.n - 1;
+    }
+    const int64_t span_a = (int64_t)round256((size_t)(hi_a - lo_a + 1) * dt_size(c0.dta));
+    const int64_t span_b = c0.kind == BK_BINARY ? (int64_t)round256((size_t)(hi_b - lo_b + 1) * dt_size(c0.dtb)) : 0;
+    const int64_t span_o = (int64_t)round256((size_t)(hi_o - lo_o + 1) * dt_size(c0.dto));
+    const int64_t per_copy = span_a + span_b + span_o;
+    if ((size_t)per_copy > TIME_POOL)
+        return set_err(IONP_ERR_UNSUPPORTED, "ionp_batch_time_call: the call's operands exceed the 1 GiB timing pool");
     cudaEvent_t e0, e1;
     if ((st = cuda_err(cudaEventCreate(&e0), "time events"))) return st;
     if ((st = cuda_err(cudaEventCreate(&e1), "time events"))) { cudaEventDestroy(e0); return st; }
     for (int k = 0; k < nsched; ++k) {
         if ((st = check_schedule(&scheds[k]))) break;
-        BatchCall c = b->calls[call];
+        BatchCall c = c0;
         tile_call(c, scheds[k]);
-        c.tile0 = 0;
         c.flags = b->d_flags + c.user_id;
         const size_t smem = row_smem(c);
         if (smem > 48 * 1024 &&
@@ -1031,51 +1099,56 @@ int32_t ionp_batch_time_call(IonpBatch* b, int32_t call, int32_t nsched, const I
         int per_sm = 1;
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch, BT_THREADS, smem);
         const int64_t slots = (int64_t)std::max(per_sm, 1) * b->sms;
-        if (c.ntiles_one > 0) {
-            c.copies = (int32_t)std::min<int64_t>(4096, std::max<int64_t>(1, ceil_div(4 * slots, c.ntiles_one)));
-            c.ntiles = c.ntiles_one * c.copies;
-        }
-        if (c.ntiles > b->one_cap) {
+        int64_t K = 1;
+        if (c.ntiles_one > 0) K = std::min<int64_t>(KMAX, std::max<int64_t>(1, ceil_div(4 * slots, c.ntiles_one)));
+        K = std::max<int64_t>(1, std::min<int64_t>(K, (int64_t)(TIME_POOL / (size_t)std::max<int64_t>(per_copy, 1))));
+        const int64_t ntiles = c.ntiles_one * K;
+        if (ntiles > b->one_cap) {
             if (b->d_one_map) scratch_free(b->d_one_map, s);
-            b->one_cap = std::max<int64_t>(c.ntiles, 4096);
+            b->one_cap = std::max<int64_t>(ntiles, 4096);
             b->d_one_map = (int32_t*)scratch_alloc(sizeof(int32_t) * b->one_cap, s);
             if (!b->d_one_map) { b->one_cap = 0; st = IONP_ERR_OOM; break; }
-            std::vector<int32_t> cyc((size_t)b->one_cap);
-            for (size_t i = 0; i < cyc.size(); ++i) cyc[i] = (int32_t)(i % NDESC);
-            if ((st = cuda_err(cudaMemcpy(b->d_one_map, cyc.data(), sizeof(int32_t) * cyc.size(), cudaMemcpyHostToDevice),
-                               "time map")))
-                break;
+        }
+        if (ntiles) {
+            k_copy_map<<<(int)std::min<int64_t>(ceil_div(ntiles, 256), 4096), 256, 0, s>>>(b->d_one_map, ntiles, c.ntiles_one);
+            count_launch();
         }
         void* part = nullptr;
-        const size_t nslot = (size_t)c.n * c.copies;
+        int64_t pstride = 0, astride = 0;
         if (c.kind != BK_BINARY && c.split > 1) {
-            part = scratch_alloc(nslot * (c.split * 8 + 4), s);
+            pstride = c.n * c.split * 8;
+            astride = c.n;
+            part = scratch_alloc((size_t)K * (size_t)(pstride + astride * 4), s);
             if (!part) { st = IONP_ERR_OOM; break; }
-            c.partial = part;
-            c.arrive = (uint32_t*)((char*)part + nslot * c.split * 8);
         }
-        const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(c.ntiles, slots));
-        BatchCall descs[NDESC];
-        for (int q = 0; q < NDESC; ++q) descs[q] = c;
-        if ((st = cuda_err(cudaMemcpyAsync(b->d_one, descs, sizeof(descs), cudaMemcpyHostToDevice, s), "time upload"))) break;
+        // template in slot KMAX, copies in slots 0..K-1
+        if ((st = cuda_err(cudaMemcpyAsync(b->d_one + KMAX, &c, sizeof(BatchCall), cudaMemcpyHostToDevice, s), "time upload")))
+            break;
+        k_replicate<<<(int)ceil_div(K, 128), 128, 0, s>>>(b->d_one + KMAX, b->d_one, (int)K, b->d_pool, span_a, span_b, span_o,
+                                                          lo_a * dt_size(c.dta), lo_b * dt_size(c.dtb), lo_o * dt_size(c.dto),
+                                                          (char*)part, pstride,
+                                                          part ? (uint32_t*)((char*)part + (size_t)K * pstride) : nullptr,
+                                                          astride);
+        count_launch();
+        const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(ntiles, slots));
         auto one = [&]() {
             cudaMemsetAsync(b->d_next, 0, 8, s);
-            if (c.arrive) cudaMemsetAsync(c.arrive, 0, nslot * 4, s);
-            if (c.ntiles) k_batch<<<grid, BT_THREADS, smem, s>>>(b->d_one, b->d_one_map, c.ntiles, b->d_next);
+            if (part) cudaMemsetAsync((char*)part + (size_t)K * pstride, 0, (size_t)K * astride * 4, s);
+            if (ntiles) k_batch<<<grid, BT_THREADS, smem, s>>>(b->d_one, b->d_one_map, ntiles, b->d_next);
             count_launch();
         };
         one();
         cudaEventRecord(e0, s);
         for (int r = 0; r < reps; ++r) one();
         cudaEventRecord(e1, s);
-        // the host copy of the descriptor and the split scratch stay alive
-        // until the runs are done
+        // the host template and the split scratch stay alive until the runs
+        // are done
         st = cuda_err(cudaEventSynchronize(e1), "time sync");
         if (part) scratch_free(part, s);
         if (st) break;
         float ms = 0;
         cudaEventElapsedTime(&ms, e0, e1);
-        us_out[k] = ms * 1000.0f / ((float)reps * (float)c.copies);
+        us_out[k] = ms * 1000.0f / ((float)reps * (float)K);
         if ((st = cuda_err(cudaGetLastError(), "time launch"))) break;
     }
     cudaEventDestroy(e0);

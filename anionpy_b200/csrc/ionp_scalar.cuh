@@ -452,7 +452,8 @@ template <class I> __device__ __forceinline__ I i_floor_div(I x, I y) {
     if (y == 0) return 0;
     if constexpr (!std::is_signed<I>::value) return (I)(x / y);
     else {
-        I q = w_div(x, y), r = w_rem(x, y);
+        // one division: r = x - q y (wrapping; also 0 for MIN / -1)
+        I q = w_div(x, y), r = w_sub<I>(x, w_mul<I>(q, y));
         if (r != 0 && ((r < 0) != (y < 0))) return w_sub<I>(q, (I)1);
         return q;
     }
@@ -461,7 +462,7 @@ template <class I> __device__ __forceinline__ I i_remainder(I x, I y) {
     if (y == 0) return 0;
     if constexpr (!std::is_signed<I>::value) return (I)(x % y);
     else {
-        I r = w_rem(x, y);
+        I r = w_sub<I>(x, w_mul<I>(w_div(x, y), y));
         if (r != 0 && ((r < 0) != (y < 0))) return w_add(r, y);
         return r;
     }

@@ -108,16 +108,16 @@ __device__ __forceinline__ double exp_first(double x, bool* ok) {
     const double tail = __fma_rn(th, tr, __fma_rn(tl, rh, tl) + (pl + sl));
     double yh, yl;
     quick_two_sum(sh, tail, &yh, &yl);
-    const double eb = yh * 0x1p-66;
+    const double eb = yh * 0x1p-65;
     const double a = yh + (yl + eb), b = yh + (yl - eb);
     *ok = a == b;
     // 2^m, m in [-1021, 1022] on the first-pass range
     return a * __longlong_as_double((long long)(1023 + m) << 52);
 }
 
-// log x = e ln2 - log(inv_j) + log1p(r), r = y inv_j - 1 exact (y = the
-// mantissa in [1, 2), inv_j a 9-bit reciprocal, |r| <= 2^-7.6), log1p(r) =
-// r + q, q to r^9/9. Near 1 (|x - 1| < 2^-7) log1p(x - 1) directly, with
+// log x = e ln2 - log(inv_j) + log1p(r), r = y inv_j - 1 as an exact
+// double-double (y = the mantissa in [1, 2), inv_j a 9-bit reciprocal,
+// |r| <= 2^-7.6), log1p(r) = r + q, q to r^9/9. Near 1 (|x - 1| < 2^-7) log1p(x - 1) directly, with
 // r^2/2 split exactly. Absolute error of y_hi + y_lo below 2^-66 (table
 // path) or |r| 2^-66 (near 1).
 __device__ __forceinline__ double log_first(double x, bool* ok) {
@@ -139,7 +139,7 @@ __device__ __forceinline__ double log_first(double x, bool* ok) {
         quick_two_sum(r, -0.5 * hh, &s, &se);
         const double tail = se + (q - 0.5 * hl);
         quick_two_sum(s, tail, &yh, &yl);
-        eb = fabs(r) * 0x1p-66;
+        eb = fabs(r) * 0x1p-65;
     } else {
         uint64_t bits = (uint64_t)__double_as_longlong(x);
         int e = 0;
@@ -152,7 +152,12 @@ __device__ __forceinline__ double log_first(double x, bool* ok) {
         const int j = (int)((bits >> 45) & 127);
         const double inv = __ldg(&LOG_INV_TAB[j]);
         const double lh = __ldg(&LOG_TAB[2 * j]), ll = __ldg(&LOG_TAB[2 * j + 1]);
-        const double r = __fma_rn(y, inv, -1.0);     // exact
+        // r = y inv - 1 as rh + rl: the product split exactly, ph - 1 exact
+        // (Sterbenz); r needs up to 54 bits, so one rounding would not do
+        const double ph = y * inv;
+        const double pl = __fma_rn(y, inv, -ph);
+        double r, rl;
+        quick_two_sum(ph - 1.0, pl, &r, &rl);
         double q = __fma_rn(r, 1.0 / 9.0, -1.0 / 8.0);
         q = __fma_rn(q, r, 1.0 / 7.0);
         q = __fma_rn(q, r, -1.0 / 6.0);
@@ -161,6 +166,7 @@ __device__ __forceinline__ double log_first(double x, bool* ok) {
         q = __fma_rn(q, r, 1.0 / 3.0);
         q = __fma_rn(q, r, -0.5);
         q = q * (r * r);                              // log1p(r) - r
+        q = q + (rl - r * rl);                        // + log1p(r + rl) - log1p(r), first order
         const double E = (double)e;
         const double ah = E * LN2_1;
         const double al = __fma_rn(E, LN2_1, -ah) + E * LN2_2;
@@ -169,15 +175,21 @@ __device__ __forceinline__ double log_first(double x, bool* ok) {
         full_two_sum(s1, r, &s2, &e2);
         const double tail = ((e1 + e2) + (al + ll)) + q;
         quick_two_sum(s2, tail, &yh, &yl);
-        eb = 0x1p-66 + fabs(yh) * 0x1p-90;
+        eb = 0x1p-65 + fabs(yh) * 0x1p-90;
     }
     const double a = yh + (yl + eb), b = yh + (yl - eb);
     *ok = a == b;
     return a;
 }
 
-static __device__ __noinline__ double exp_slow(double x) { return dd::exp_dd(x).hi; }
-static __device__ __noinline__ double log_slow(double x) { return dd::log_dd(x).hi; }
+static __device__ __noinline__ double exp_slow(double x) {
+    const dd::D2 r = dd::exp_dd(x);
+    return r.hi + r.lo;  // the correctly rounded sum, also when hi is not
+}
+static __device__ __noinline__ double log_slow(double x) {
+    const dd::D2 r = dd::log_dd(x);
+    return r.hi + r.lo;  // the correctly rounded sum, also when hi is not
+}
 
 __device__ __forceinline__ double cr_exp(double x) {
     if (isnan_d(x)) return quiet_d(x);
@@ -206,9 +218,10 @@ __device__ __forceinline__ double cr_log(double x) {
 // pairs and |b| <= 1/128:
 //   sin(a + b) = S + C b + [S (cos b - 1) + C (sin b - b)]
 //   cos(a + b) = C - S b + [C (cos b - 1) - S (sin b - b)]
-// with the products C b, S b split exactly and the bracketed tails (below
-// 2^-14 relative) in double. Error of y_hi + y_lo below 2^-66 absolute (and
-// below 2^-62 relative when a = 0), plus the reduction error.
+// with the products C b, S b split exactly, the bracketed tails (below
+// 2^-14 relative) in double and the first-order effect of b's low part on
+// them kept. Error of y_hi + y_lo below about 2^-66 absolute, tested against
+// 2^-64 (and 2^-62 relative when a = 0), plus the reduction error.
 __device__ __forceinline__ double sin_first(double x, bool* ok) {
     constexpr double TWO_OVER_PI = 0.63661977236758134308;
     const double k = rint(x * TWO_OVER_PI);
@@ -240,16 +253,17 @@ __device__ __forceinline__ double sin_first(double x, bool* ok) {
         const double ph = ch * bh;
         const double pl = __fma_rn(ch, bh, -ph);
         full_two_sum(sh, ph, &s1, &e1);
-        tail = (e1 + pl) + ((ch * bl + cl * bh) + sl) + (sh * cbm + ch * sbt);
+        // ... - S b bl: the first-order effect of bl on S (cos b - 1)
+        tail = (e1 + pl) + ((ch * bl + cl * bh) + sl) + ((sh * cbm + ch * sbt) - sh * (bh * bl));
     } else {              // cos r
         const double ph = sh * bh;
         const double pl = __fma_rn(sh, bh, -ph);
         full_two_sum(ch, -ph, &s1, &e1);
-        tail = (e1 - pl) + (cl - (sh * bl + sl * bh)) + (ch * cbm - sh * sbt);
+        tail = (e1 - pl) + (cl - (sh * bl + sl * bh)) + ((ch * cbm - sh * sbt) - ch * (bh * bl));
     }
     double yh, yl;
     quick_two_sum(s1, tail, &yh, &yl);
-    const double eb = (i == 0 && (q & 1) == 0 ? fabs(yh) * 0x1p-62 : 0x1p-66) + fabs(k) * 0x1p-103 + 0x1p-104;
+    const double eb = (i == 0 && (q & 1) == 0 ? fabs(yh) * 0x1p-62 : 0x1p-64) + fabs(k) * 0x1p-103 + 0x1p-104;
     const double a = yh + (yl + eb), b = yh + (yl - eb);
     *ok = a == b;
     // sin x = sin r, cos r, -sin r, -cos r for q = 0..3; sin(-r) = -sin r
@@ -257,7 +271,10 @@ __device__ __forceinline__ double sin_first(double x, bool* ok) {
     return flip ? -a : a;
 }
 
-static __device__ __noinline__ double sin_slow(double x) { return dd::sin_dd(x).hi; }
+static __device__ __noinline__ double sin_slow(double x) {
+    const dd::D2 r = dd::sin_dd(x);
+    return r.hi + r.lo;
+}
 
 __device__ __forceinline__ double cr_sin(double x) {
     if (isnan_d(x)) return quiet_d(x);

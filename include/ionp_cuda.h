@@ -217,10 +217,13 @@ int32_t ionp_batch_fpe(IonpBatch* b, uint32_t* words, IonpStream stream);
 /* info[0] calls, [1] tiles, [2] grid, [3] dynamic shared bytes,
  * [4] algorithmic bytes of one run */
 int32_t ionp_batch_info(IonpBatch* b, int64_t* info);
-/* Device microseconds of one call under each schedule, with the GPU
- * saturated as in a batch (the autotuner's measurement): the call is queued
- * enough times in one launch for four tiles per resident CTA (at most 4096
- * copies), reps launches run between two events; time per copy. */
+/* Device microseconds of one call under each schedule as a batch sees it
+ * (the autotuner's measurement): the call is queued enough times in one
+ * launch for four tiles per resident CTA (at most 4096 copies, all fitting a
+ * 1 GiB pool), each copy on its own operand region of the pool, so copies
+ * stream from HBM like distinct calls; reps launches between two events;
+ * time per copy. Only shapes, strides and dtypes matter: the pool's
+ * contents are arbitrary. */
 int32_t ionp_batch_time_call(IonpBatch* b, int32_t call, int32_t nsched, const IonpSchedule* scheds, int32_t reps,
                              float* us_out, IonpStream stream);
 
