@@ -8,6 +8,7 @@
 #include <vector>
 #include "ionp_host.h"
 #include "ionp_reduce_launch.cuh"
+#include "ionp_reduce_rowst.cuh"
 
 namespace ionp {
 namespace {
@@ -92,8 +93,14 @@ int32_t run_row(RedDesc& d, cudaStream_t s) {
     if (w > SEG_MAX) {
         while (*seg_lengths(w, K).rbegin() > SEG_MAX) ++K;
     }
-    // more CTAs when there are few outputs and long runs
-    while ((d.nout << K) < 148 * 2 && *seg_lengths(w, K + 1).begin() >= 4096 && K < 20) ++K;
+    // more parallel units when there are few outputs and long runs: the
+    // wide-row kernels take a warp (float add) or a CTA per unit
+    int64_t want = 148 * 2;
+    if (row_wide_ok(d, dt_bytes(d.cd))) {
+        if (rowst_type_ok(d.op, d.cd)) want = 148 * 16;
+        else if (rowco_type_ok(d.op, d.cd)) want = 148 * RCO_CTAS;
+    }
+    while ((d.nout << K) < want && *seg_lengths(w, K + 1).begin() >= 4096 && K < 20) ++K;
     auto lens = seg_lengths(w, K);
     int64_t maxlen = *lens.rbegin();
     std::map<int64_t, int> memo;
@@ -381,6 +388,23 @@ int32_t ionp_reduce(int32_t op, const IonpArr* a_in, const int32_t* axes, int32_
         }
     }
     if ((st = set_narrow(fold_axes))) { cleanup(); return st; }
+    if (red_assoc(op, cd) && d.nr == 1 && d.adt == d.cd) {
+        // too few outputs for one thread each to keep HBM busy: cut the
+        // axis into 2^K parts and fold the parts in order on top
+        int K = 0;
+        while (d.nout < 65536 && (d.nout << K) < 148 * 2048 && (d.rshape[0] >> (K + 1)) >= 256 && K < 10) ++K;
+        if (K > 0) {
+            d.K = K;
+            void* scratch = scratch_alloc((size_t)(d.nout << K) * dt_bytes(cd), s);
+            if (!scratch) { cleanup(); return IONP_ERR_OOM; }
+            d.scratch = scratch;
+            st = cuda_err(launch_reduce_col_split(d, s), "reduce col split launch");
+            if (!st) st = cuda_err(launch_reduce_row_top(d, s), "reduce col top launch");
+            scratch_free(scratch, s);
+            cleanup();
+            return st;
+        }
+    }
     st = cuda_err(launch_reduce_col(d, s), "reduce col launch");
     cleanup();
     return st;
@@ -436,6 +460,9 @@ int32_t ionp_argext(int32_t is_max, const IonpArr* a, int32_t axis, int32_t keep
         for (int i = 0; i < nd; ++i) if (i != axis && a->shape[i] > 1) min_kept = std::min<int64_t>(min_kept, std::llabs(a->strides[i]));
         if (std::llabs(d.ws) > min_kept && d.nout >= 148 * 32) mode = 1;  // column scan
     }
+    if (mode == 0 && axis != -1 && d.nr == 1 && d.ws == 1 && d.nk == 1 && d.kst[0] == d.w && d.nout >= 148 * 256 &&
+        (d.w * dt_bytes(d.cd)) % 16 == 0 && d.w * dt_bytes(d.cd) <= 256 && reinterpret_cast<uintptr_t>(d.a) % 16 == 0)
+        return cuda_err(launch_argext(d, is_max, 3, tpr, s), "argext narrow launch");
     if (mode == 0) {
         tpr = d.w < 64 ? 1 : d.w <= 4096 ? 32 : 256;
         int K = 0;
@@ -453,7 +480,20 @@ int32_t ionp_argext(int32_t is_max, const IonpArr* a, int32_t axis, int32_t keep
         if (scratch) scratch_free(scratch, s);
         return st;
     }
-    return cuda_err(launch_argext(d, is_max, 1, tpr, s), "argext col launch");
+    // column scan; split the axis when the outputs alone leave HBM idle
+    int K = 0;
+    while ((d.nout << K) < 148 * 2048 && (d.w >> (K + 1)) >= 256 && K < 10) ++K;
+    d.K = K;
+    void* scratch = nullptr;
+    if (K > 0) {
+        scratch = scratch_alloc((size_t)(d.nout << K) * (dt_bytes(d.cd) + 8) + 64, s);
+        if (!scratch) return IONP_ERR_OOM;
+        d.scratch = scratch;
+    }
+    st = cuda_err(launch_argext(d, is_max, 1, tpr, s), "argext col launch");
+    if (!st && K > 0) st = cuda_err(launch_argext(d, is_max, 2, tpr, s), "argext top launch");
+    if (scratch) scratch_free(scratch, s);
+    return st;
 }
 
 }  // extern "C"

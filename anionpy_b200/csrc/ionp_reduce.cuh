@@ -74,6 +74,7 @@ struct RedDesc {
     // split ROW (K > 0): partials scratch, nout x 2^K accumulators
     int32_t K;
     int32_t D;       // slot-tree depth of one segment
+    int32_t Dw, Dl;  // wide-row staged kernel: window depth, leaf-slot depth
     void* scratch;
     // masked
     const uint8_t* m;
@@ -135,6 +136,13 @@ template <int OP, int CD, bool CASTLD = false> struct RPol {
         }
     }
 };
+
+// IEEE add without the NaN payload rule: equal to the engine's add whenever
+// the result is not NaN.
+template <class T> __device__ __forceinline__ T plain_sum(T x, T y) {
+    if constexpr (sizeof(T) == 8) return __dadd_rn(x, y);
+    else return __fadd_rn(x, y);
+}
 
 __host__ __device__ __forceinline__ int64_t pw_split(int64_t len) {
     int64_t n2 = len / 2;
@@ -414,11 +422,14 @@ __global__ void __launch_bounds__(RED_THREADS) k_red_row_top(RedDesc d) {
     }
 }
 
-// COL kernel: sequential fold per output over the narrow dims (fold order).
-template <int OP, int CD, bool CASTLD>
+// COL kernel: sequential fold per output over the narrow dims (fold order),
+// U loads in flight per thread (64 when the outputs are too few for 16 to
+// keep HBM busy).
+template <int OP, int CD, bool CASTLD, int U = 16>
 __global__ void __launch_bounds__(RED_THREADS) k_red_col(RedDesc d) {
     typedef typename DT<CD>::T T;
     typedef RPol<OP, CD, CASTLD> P;
+    constexpr bool FADD = OP == OP_ADD && (CD == DT_F32 || CD == DT_F64);
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     int64_t total = 1;
     for (int k = 0; k < d.nr; ++k) total *= d.rshape[k];
@@ -436,7 +447,12 @@ __global__ void __launch_bounds__(RED_THREADS) k_red_col(RedDesc d) {
         for (int64_t done = 0; done < total; done += rn_in) {
             const int64_t b0 = base + outer_off;
             int64_t j = 0;
-            constexpr int U = 16;
+            if (!have && rn_in > 0) {
+                if constexpr (CASTLD) acc = load_int_widen<CD>(d.a, b0, d.adt);
+                else acc = ((const T*)d.a)[b0];
+                have = true;
+                j = 1;
+            }
             for (; j + U <= rn_in; j += U) {
                 T x[U];
 #pragma unroll
@@ -444,10 +460,26 @@ __global__ void __launch_bounds__(RED_THREADS) k_red_col(RedDesc d) {
                     if constexpr (CASTLD) x[u] = load_int_widen<CD>(d.a, b0 + (j + u) * rs_in, d.adt);
                     else x[u] = ((const T*)d.a)[b0 + (j + u) * rs_in];
                 }
+                if constexpr (FADD) {
+                    // plain adds; a NaN result replays the block with the
+                    // engine's NaN rule; once the sum is a quiet NaN no
+                    // later add changes it
+                    if (acc == acc) {
+                        T r = acc;
 #pragma unroll
-                for (int u = 0; u < U; ++u) {
-                    if (!have) { acc = x[u]; have = true; }
-                    else acc = BinOp<OP, CD>::apply(acc, x[u]);
+                        for (int u = 0; u < U; ++u) r = plain_sum(r, x[u]);
+                        if (r != r) {
+                            r = acc;
+#pragma unroll
+                            for (int u = 0; u < U; ++u) r = BinOp<OP, CD>::apply(r, x[u]);
+                        }
+                        acc = r;
+                    } else {
+                        acc = BinOp<OP, CD>::apply(acc, x[0]);  // quiets a signaling NaN once
+                    }
+                } else {
+#pragma unroll
+                    for (int u = 0; u < U; ++u) acc = BinOp<OP, CD>::apply(acc, x[u]);
                 }
             }
             for (; j < rn_in; ++j) {
@@ -466,6 +498,39 @@ __global__ void __launch_bounds__(RED_THREADS) k_red_col(RedDesc d) {
             }
         }
         store_cast<CD>(d.o, out_off, d.odt, acc);
+    }
+}
+
+// COL kernel, split: one narrow axis folded by an order-free (associative)
+// op. Too few outputs to keep HBM busy with one thread each, so the axis is
+// cut into 2^K contiguous parts; task t folds part t / nout of output
+// t % nout (adjacent threads, adjacent outputs) in order with 16 loads in
+// flight, and k_red_row_top folds the parts in order and applies the seed.
+template <int OP, int CD>
+__global__ void __launch_bounds__(RED_THREADS) k_red_col_split(RedDesc d) {
+    typedef typename DT<CD>::T T;
+    const int64_t P = (int64_t)1 << d.K;
+    const int64_t len = d.rshape[0], rs = d.rst[0];
+    const int64_t ntask = d.nout * P;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < ntask; t += stride) {
+        const int64_t part = t / d.nout, o = t - part * d.nout;
+        int64_t base, out_off;
+        kept_offsets(d, o, &base, &out_off);
+        const int64_t r0 = part * len / P, r1 = (part + 1) * len / P;
+        const T* p = (const T*)d.a + base;
+        T acc = p[r0 * rs];
+        int64_t j = r0 + 1;
+        constexpr int U = 16;
+        for (; j + U <= r1; j += U) {
+            T x[U];
+#pragma unroll
+            for (int u = 0; u < U; ++u) x[u] = p[(j + u) * rs];
+#pragma unroll
+            for (int u = 0; u < U; ++u) acc = BinOp<OP, CD>::apply(acc, x[u]);
+        }
+        for (; j < r1; ++j) acc = BinOp<OP, CD>::apply(acc, p[j * rs]);
+        reinterpret_cast<T*>(d.scratch)[o * P + part] = acc;
     }
 }
 
@@ -540,8 +605,26 @@ __global__ void __launch_bounds__(RED_THREADS, COLST_CTAS) k_red_col_staged(RedD
                     T x[8];
 #pragma unroll
                     for (int u = 0; u < 8; ++u) x[u] = sb[(r + u) * COLS];
+                    if constexpr (OP == OP_ADD && (CD == DT_F32 || CD == DT_F64)) {
+                        // plain adds, replayed with the NaN rule only when
+                        // the block's sum turns NaN; a NaN sum stays as is
+                        if (acc == acc) {
+                            T t = acc;
 #pragma unroll
-                    for (int u = 0; u < 8; ++u) acc = BinOp<OP, CD>::apply(acc, x[u]);
+                            for (int u = 0; u < 8; ++u) t = plain_sum(t, x[u]);
+                            if (t != t) {
+                                t = acc;
+#pragma unroll
+                                for (int u = 0; u < 8; ++u) t = BinOp<OP, CD>::apply(t, x[u]);
+                            }
+                            acc = t;
+                        } else {
+                            acc = BinOp<OP, CD>::apply(acc, x[0]);  // quiets a signaling NaN once
+                        }
+                    } else {
+#pragma unroll
+                        for (int u = 0; u < 8; ++u) acc = BinOp<OP, CD>::apply(acc, x[u]);
+                    }
                 }
                 for (; r < nr; ++r) acc = BinOp<OP, CD>::apply(acc, sb[r * COLS]);
             }
@@ -941,8 +1024,91 @@ __global__ void __launch_bounds__(RED_THREADS) k_argext(RedDesc d) {
     }
 }
 
+// Top of a split scan: one CTA per output combines its 2^K (value, index)
+// partials. `takes` keeps the better value and, between equals (or two
+// NaNs), the smaller index, so any combine order gives the sequential scan's
+// answer; threads take strided partials, then a shuffle and a shared-memory
+// tree finish.
 template <int CD, bool MAX>
-__global__ void k_argext_top(RedDesc d) {
+__global__ void __launch_bounds__(RED_THREADS) k_argext_top(RedDesc d) {
+    typedef ArgPol<CD, MAX> P;
+    typedef typename DT<CD>::T T;
+    __shared__ T sv[RED_THREADS / 32];
+    __shared__ int64_t si[RED_THREADS / 32];
+    const int64_t nseg = (int64_t)1 << d.K;
+    const int64_t ntasks = d.nout * nseg;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int64_t o = blockIdx.x; o < d.nout; o += gridDim.x) {
+        const int64_t* ix = reinterpret_cast<const int64_t*>(d.scratch) + o * nseg;
+        const T* v = reinterpret_cast<const T*>(reinterpret_cast<const int64_t*>(d.scratch) + ntasks) + o * nseg;
+        T best{};
+        int64_t bi = -1;
+        for (int64_t s = threadIdx.x; s < nseg; s += RED_THREADS)
+            if (P::takes(v[s], ix[s], best, bi)) { best = v[s]; bi = ix[s]; }
+#pragma unroll
+        for (int h = 16; h >= 1; h >>= 1) {
+            T ov = __shfl_down_sync(0xffffffffu, best, h);
+            int64_t oi = __shfl_down_sync(0xffffffffu, bi, h);
+            if (P::takes(ov, oi, best, bi)) { best = ov; bi = oi; }
+        }
+        if (lane == 0) { sv[warp] = best; si[warp] = bi; }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            for (int w = 1; w < RED_THREADS / 32; ++w)
+                if (P::takes(sv[w], si[w], best, bi)) { best = sv[w]; bi = si[w]; }
+            int64_t in_off, out_off;
+            kept_offsets(d, o, &in_off, &out_off);
+            ((int64_t*)d.o)[out_off] = bi < 0 ? 0 : bi;
+        }
+        __syncthreads();
+    }
+}
+
+// Column-order argext: one output per thread, sequential over the axis;
+// with d.K > 0 the axis is cut into 2^K contiguous parts (task t scans part
+// t / nout of output t % nout) whose (value, index) partials k_argext_top
+// combines.
+template <int CD, bool MAX>
+__global__ void __launch_bounds__(RED_THREADS) k_argext_col(RedDesc d) {
+    typedef ArgPol<CD, MAX> P;
+    typedef typename DT<CD>::T T;
+    const int64_t nseg = (int64_t)1 << d.K;
+    const int64_t ntask = d.nout * nseg;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < ntask; t += stride) {
+        const int64_t part = t / d.nout, o = t - part * d.nout;
+        int64_t base, out_off;
+        kept_offsets(d, o, &base, &out_off);
+        const int64_t r0 = part * d.w / nseg, r1 = (part + 1) * d.w / nseg;
+        const T* p = (const T*)d.a + base;
+        T best = p[r0 * d.ws];
+        int64_t bi = r0;
+        int64_t i = r0 + 1;
+        constexpr int U = 16;
+        for (; i + U <= r1; i += U) {
+            T x[U];
+#pragma unroll
+            for (int u = 0; u < U; ++u) x[u] = p[(i + u) * d.ws];
+#pragma unroll
+            for (int u = 0; u < U; ++u) if (P::better(x[u], best)) { best = x[u]; bi = i + u; }
+        }
+        for (; i < r1; ++i) {
+            T x = p[i * d.ws];
+            if (P::better(x, best)) { best = x; bi = i; }
+        }
+        if (d.K == 0) {
+            ((int64_t*)d.o)[out_off] = bi;
+        } else {
+            int64_t* ixs = reinterpret_cast<int64_t*>(d.scratch);
+            reinterpret_cast<T*>(ixs + ntask)[o * nseg + part] = best;
+            ixs[o * nseg + part] = bi;
+        }
+    }
+}
+
+// Top of a split scan with few partials per output: one thread per output.
+template <int CD, bool MAX>
+__global__ void __launch_bounds__(RED_THREADS) k_argext_top_small(RedDesc d) {
     typedef ArgPol<CD, MAX> P;
     typedef typename DT<CD>::T T;
     const int64_t nseg = (int64_t)1 << d.K;
@@ -952,48 +1118,77 @@ __global__ void k_argext_top(RedDesc d) {
         const T* v = reinterpret_cast<const T*>(reinterpret_cast<const int64_t*>(d.scratch) + ntasks) + o * nseg;
         T best{};
         int64_t bi = -1;
-        for (int64_t s = 0; s < nseg; ++s) {
+        for (int64_t s = 0; s < nseg; ++s)
             if (P::takes(v[s], ix[s], best, bi)) { best = v[s]; bi = ix[s]; }
-        }
         int64_t in_off, out_off;
         kept_offsets(d, o, &in_off, &out_off);
         ((int64_t*)d.o)[out_off] = bi < 0 ? 0 : bi;
     }
 }
 
-// Column-order argext: one output per thread, sequential over the axis.
+// Argext over many short C-contiguous rows (16..256 bytes each): the
+// staged ring and swizzle of k_red_rownar, one thread scanning one row in
+// index order.
 template <int CD, bool MAX>
-__global__ void __launch_bounds__(RED_THREADS) k_argext_col(RedDesc d) {
+__global__ void __launch_bounds__(RED_THREADS, 2) k_argext_nar(RedDesc d) {
     typedef ArgPol<CD, MAX> P;
     typedef typename DT<CD>::T T;
-    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-    for (int64_t o = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; o < d.nout; o += stride) {
-        int64_t base, out_off;
-        kept_offsets(d, o, &base, &out_off);
-        const T* p = (const T*)d.a + base;
-        T best = p[0];
-        int64_t bi = 0;
-        int64_t i = 1;
-        constexpr int U = 16;
-        for (; i + U <= d.w; i += U) {
-            T x[U];
-#pragma unroll
-            for (int u = 0; u < U; ++u) x[u] = p[(i + u) * d.ws];
-#pragma unroll
-            for (int u = 0; u < U; ++u) if (P::better(x[u], best)) { best = x[u]; bi = i + u; }
+    constexpr int VE = 16 / (int)sizeof(T);
+    constexpr int STAGES = 3;
+    constexpr int WCH = 32768 / 16;  // 16-byte chunks per stage
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    uint4* ring = reinterpret_cast<uint4*>(smem_raw);
+    const int w = (int)d.w;
+    const int m = w / VE;
+    const int R = WCH / m < 2048 ? WCH / m : 2048;
+    const int64_t nwin = (d.nout + R - 1) / R;
+    const int64_t myw = nwin > blockIdx.x ? (nwin - blockIdx.x + gridDim.x - 1) / gridDim.x : 0;
+    const uint4* a = reinterpret_cast<const uint4*>(d.a);
+    auto swz = [](int g) { return g ^ ((g >> 3) & 7); };
+    auto issue = [&](int64_t q) {
+        if (q < myw) {
+            const int64_t r0 = (blockIdx.x + q * (int64_t)gridDim.x) * R;
+            const int64_t rows = d.nout - r0 < R ? d.nout - r0 : R;
+            const int nch = (int)rows * m;
+            uint4* sb = ring + (size_t)(q % STAGES) * WCH;
+            const uint4* src = a + r0 * m;
+            for (int c = threadIdx.x; c < nch; c += RED_THREADS) cp_async16(sb + swz(c), src + c);
         }
-        for (; i < d.w; ++i) {
-            T x = p[i * d.ws];
-            if (P::better(x, best)) { best = x; bi = i; }
+        cp_async_commit();
+    };
+    for (int s = 0; s < STAGES - 1; ++s) issue(s);
+    for (int64_t q = 0; q < myw; ++q) {
+        issue(q + STAGES - 1);
+        cp_async_wait<STAGES - 1>();
+        __syncthreads();
+        const int64_t r0 = (blockIdx.x + q * (int64_t)gridDim.x) * R;
+        const int rows = (int)(d.nout - r0 < R ? d.nout - r0 : R);
+        const uint4* sb = ring + (size_t)(q % STAGES) * WCH;
+        for (int r = threadIdx.x; r < rows; r += RED_THREADS) {
+            const int g0 = r * m;
+            T best{};
+            int bi = 0;
+            for (int c = 0; c < m; ++c) {
+                uint4 v = sb[swz(g0 + c)];
+                T x[VE];
+                memcpy(x, &v, 16);
+#pragma unroll
+                for (int i = 0; i < VE; ++i) {
+                    if ((c == 0 && i == 0) || P::better(x[i], best)) { best = x[i]; bi = c * VE + i; }
+                }
+            }
+            ((int64_t*)d.o)[(r0 + r) * d.kost[0]] = bi;  // one kept dim
         }
-        ((int64_t*)d.o)[out_off] = bi;
+        __syncthreads();
     }
+    cp_async_wait<0>();
 }
 
 // Launchers (ionp_reduce.cu)
 cudaError_t launch_reduce_row(const RedDesc& d, int tpr, size_t smem, int grid, cudaStream_t s);
 cudaError_t launch_reduce_row_top(const RedDesc& d, cudaStream_t s);
 cudaError_t launch_reduce_col(const RedDesc& d, cudaStream_t s);
+cudaError_t launch_reduce_col_split(const RedDesc& d, cudaStream_t s);
 cudaError_t launch_reduce_gen(const RedDesc& d, cudaStream_t s);
 cudaError_t launch_reduce_masked(const RedDesc& d, cudaStream_t s);
 cudaError_t launch_argext(const RedDesc& d, int is_max, int mode, int tpr, cudaStream_t s);

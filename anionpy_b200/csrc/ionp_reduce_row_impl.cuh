@@ -2,6 +2,7 @@
 // translation units ionp_reduce_row_*.cu.
 #pragma once
 #include "ionp_reduce_launch.cuh"
+#include "ionp_reduce_rowst.cuh"
 
 namespace ionp {
 
@@ -9,6 +10,10 @@ constexpr bool red_castld_ok(int op, int cd) { return (op == OP_ADD || op == OP_
 
 template <int OP, int CD, bool C>
 static cudaError_t row_t2(const RedDesc& d, int tpr, size_t smem, int grid, cudaStream_t s) {
+    if constexpr (!C) {
+        cudaError_t e = launch_row_wide<OP, CD>(d, s);
+        if (e != cudaErrorNotSupported) return e;
+    }
     switch (tpr) {
         case 1: k_red_row<OP, CD, 1, C><<<grid, RED_THREADS, smem, s>>>(d); break;
         case 32: k_red_row<OP, CD, 32, C><<<grid, RED_THREADS, smem, s>>>(d); break;

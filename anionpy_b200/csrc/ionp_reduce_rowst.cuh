@@ -1,0 +1,660 @@
+// Wide-row reduction kernels for contiguous 4- and 8-byte runs: the common
+// case of ufunc.reduce over the last axis (or over all axes) of a C-ordered
+// array. They replace k_red_row's thread-per-leaf loads, where every lane of
+// a warp reads 16 bytes of a different 512-byte leaf, by loads in which a
+// warp touches whole 128-byte lines.
+//
+//  k_red_rowst : float add, numpy's pairwise tree (ufunc.rs:6416-6448).
+//                Each run segment is cut at a fixed depth Dw of its split
+//                tree into windows of at most 16 KiB; a window is a subtree,
+//                so its leaves never cross a window edge. cp.async streams
+//                windows into a 4-stage shared-memory ring (every 128-element
+//                leaf block padded by 8 elements, so that the 8 lanes that
+//                sum one leaf's 8 interleaved accumulators and the 4 leaves
+//                a warp sums at once fall in distinct banks). Eight lanes sum
+//                one leaf: lane k folds accumulator k (elements k, k+8, ...)
+//                in order, the group combines ((r0+r1)+(r2+r3))+((r4+r5)+
+//                (r6+r7)) with shuffles and lane 0 adds the len % 8 tail.
+//                Leaf sums go to a perfect-binary-tree slot array that warp 0
+//                folds level by level with shuffles (left operand first);
+//                window sums go to the segment's slot array, folded the same
+//                way after its last window.
+//  k_red_rowco : the order-free folds: integer add/multiply (wrapping),
+//                bitwise and/or/xor, integer max/min, and float max/min,
+//                whose only order dependence is that the first NaN in fold
+//                order is the result (float_max/float_min return an operand
+//                unchanged, and their non-NaN results do not depend on the
+//                order, +0 winning a maximum tie and -0 a minimum tie). Lane l
+//                of a warp reads 16 bytes at offset 16*l of each 512-byte
+//                chunk (4 chunks in flight), folds them into its own
+//                accumulator and remembers its first NaN with its index; the
+//                accumulators meet in a warp and then a CTA tree, where the
+//                NaN with the smallest index wins.
+//
+// Both take the segments of the K-level split of run_row (nout x 2^K units)
+// and write either the output (K == 0) or one partial per unit for
+// k_red_row_top.
+#pragma once
+#include "ionp_reduce.cuh"
+
+#include <algorithm>
+#include <map>
+#include <set>
+
+namespace ionp {
+
+constexpr int RST_WIN = 4096;         // elements per window (a subtree of the split tree)
+constexpr int RST_STAGES = 2;         // per-warp ring depth
+constexpr int RST_MAXDW = 6;          // at most 64 windows per segment
+constexpr int RST_MAXDL = 6;          // at most 64 leaves per window (two per lane)
+constexpr int RCO_CTAS = 5;
+constexpr int RCO_U = 4;              // 512-byte chunks in flight per warp
+
+// 16 bytes of padding after every 128 elements: one lane per 128-element
+// leaf, so the lanes of a 16-byte shared load sit 4 banks apart
+template <class T> constexpr int rst_pad() { return 16 / (int)sizeof(T); }
+template <class T> constexpr int rst_win_phys() { return RST_WIN + rst_pad<T>() * (RST_WIN / 128); }
+template <class T> constexpr int rst_warps() { return sizeof(T) == 4 ? 2 : 1; }  // warps per CTA
+// window element e sits at e + pad * (e / 128) in the stage buffer
+template <class T> __device__ __forceinline__ int rst_phys(int e) { return e + rst_pad<T>() * (e >> 7); }
+
+
+__device__ __forceinline__ int pw_split32(int len) {
+    int n2 = len / 2;
+    return n2 - n2 % 8;
+}
+
+// Node `p` at depth Dw of the split tree of a segment of `len` elements;
+// false when a leaf (<= 128 elements) closes the path above Dw and p is not
+// the first path through it.
+__device__ __forceinline__ bool rst_node(int64_t len, int Dw, int p, int64_t* off, int* nlen) {
+    int64_t o = 0, l = len;
+    for (int k = Dw - 1; k >= 0; --k) {
+        if (l <= PW_BLOCK) {
+            if (p & ((1 << (k + 1)) - 1)) return false;
+            break;
+        }
+        int64_t n2 = pw_split(l);
+        if ((p >> k) & 1) { o += n2; l -= n2; } else { l = n2; }
+    }
+    *off = o;
+    *nlen = (int)l;
+    return true;
+}
+
+template <class T> __device__ __forceinline__ void cp_async_elem(T* smem, const T* gmem) {
+    unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+    if constexpr (sizeof(T) == 8) asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(gmem) : "memory");
+    else asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+
+// Warp 0 folds a perfect-binary-tree slot array of 2^D <= 64 entries (lane l
+// holds slots 2l and 2l+1); the root lands in lane 0. A right subtree exists
+// only where its left sibling does, so a missing right operand leaves the
+// left one unchanged.
+template <class P>
+__device__ __forceinline__ typename P::A warp_slot_tree(const typename P::A* s, const uint8_t* v, int D, int lane) {
+    typedef typename P::A A;
+    const int ns = 1 << D;
+    const int i0 = 2 * lane, i1 = i0 + 1;
+    A a{};
+    int va = 0;
+    if (i0 < ns && v[i0]) { a = s[i0]; va = 1; }
+    if (i1 < ns && v[i1]) a = P::fold(a, s[i1]);
+#pragma unroll
+    for (int h = 1; h < 32; h <<= 1) {
+        A pa = __shfl_down_sync(0xffffffffu, a, h);
+        int pv = __shfl_down_sync(0xffffffffu, va, h);
+        if ((lane & (2 * h - 1)) == 0 && pv && va) a = P::fold(a, pa);
+    }
+    return a;
+}
+
+// Per-stage description of a window, written by the warp that issued its
+// copies and read back when the warp folds it.
+struct RstMeta {
+    int64_t unit;
+    int len, p, live, pad;
+};
+
+// Plain IEEE add (no NaN payload rule): equal to the engine's add whenever
+// the result is not NaN.
+template <class T> __device__ __forceinline__ T plain_add(T x, T y) {
+    if constexpr (sizeof(T) == 8) return __dadd_rn(x, y);
+    else return __fadd_rn(x, y);
+}
+
+// Per-warp shared memory of k_red_rowst: the window ring, the segment's
+// window-sum slots, one window's leaf-sum slots, the ring's descriptions.
+template <class T> constexpr size_t rst_warp_smem() {
+    return ((size_t)RST_STAGES * rst_win_phys<T>() * sizeof(T) + 64 * sizeof(T) * 2 +
+            (size_t)RST_STAGES * sizeof(RstMeta) + 64 * 2 + 127) / 128 * 128;  // each warp's ring 128-byte aligned
+}
+template <class T> constexpr size_t rst_smem() { return (size_t)rst_warps<T>() * rst_warp_smem<T>(); }
+
+template <int OP, int CD>
+__global__ void __launch_bounds__(32 * rst_warps<typename DT<CD>::T>()) k_red_rowst(RedDesc d) {
+    typedef RPol<OP, CD> P;
+    typedef typename P::A A;
+    typedef typename DT<CD>::T T;
+    static_assert(sizeof(A) == sizeof(T), "no widening in the staged kernel");
+    constexpr int VE = 16 / (int)sizeof(T);
+    constexpr int PADE = rst_pad<T>();
+    constexpr int WP = rst_win_phys<T>();
+    constexpr int NWARP = rst_warps<T>();
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    unsigned char* mine = smem_raw + (size_t)warp * rst_warp_smem<T>();
+    T* ring = reinterpret_cast<T*>(mine);
+    A* uslot = reinterpret_cast<A*>(ring + (size_t)RST_STAGES * WP);   // [64]
+    A* lslot = uslot + 64;                                               // [64]
+    RstMeta* meta = reinterpret_cast<RstMeta*>(lslot + 64);              // [RST_STAGES]
+    uint8_t* uvalid = reinterpret_cast<uint8_t*>(meta + RST_STAGES);     // [64]
+    uint8_t* lvalid = uvalid + 64;                                       // [64]
+    const int Dw = d.Dw, Dl = d.Dl, NW = 1 << Dw;
+    const int64_t nseg = (int64_t)1 << d.K;
+    const int64_t nunits = d.nout * nseg;
+    const int64_t gw = (int64_t)blockIdx.x * NWARP + warp, GW = (int64_t)gridDim.x * NWARP;
+    const int64_t myunits = nunits > gw ? (nunits - gw + GW - 1) / GW : 0;
+    const int64_t Q = myunits * NW;
+    for (int i = lane; i < 64; i += 32) { uvalid[i] = 0; lvalid[i] = 0; }
+    const T* a = reinterpret_cast<const T*>(d.a);
+
+    // the segment of the unit last issued (cached across its windows)
+    int64_t cu = -1, cbase = 0, clen = 0;
+    auto issue = [&](int64_t q) {
+        if (q < Q) {
+            const int64_t u = gw + (q >> Dw) * GW;
+            const int p = (int)(q & (NW - 1));
+            if (u != cu) {
+                int64_t in_off, out_off, soff;
+                kept_offsets(d, u >> d.K, &in_off, &out_off);
+                seg_of(d.w, d.K, u & (nseg - 1), &soff, &clen);
+                cbase = in_off + soff;
+                cu = u;
+            }
+            int64_t noff = 0;
+            int nlen = 0;
+            const bool live = rst_node(clen, Dw, p, &noff, &nlen);
+            if (live) {
+                T* sb = ring + (size_t)(q % RST_STAGES) * WP;
+                const T* src = a + cbase + noff;
+                const int nch = nlen / VE;
+                for (int c = lane; c < nch; c += 32) cp_async16(sb + rst_phys<T>(c * VE), src + c * VE);
+                for (int e = nch * VE + lane; e < nlen; e += 32) cp_async_elem(sb + rst_phys<T>(e), src + e);
+            }
+            if (lane == 0) {
+                RstMeta& m = meta[q % RST_STAGES];
+                m.unit = u;
+                m.len = nlen;
+                m.p = p;
+                m.live = live;
+            }
+        }
+        cp_async_commit();  // one group per window, empty or not
+    };
+    // the leaves that start at this lane's two candidate positions (2*lane
+    // and 2*lane + 1, 64 elements apart) for the current window length: one
+    // 128-element leaf per lane in a regular window
+    int cachedL = -1;
+    int loff[2], llen[2], lsi[2];
+    bool lhas[2];
+    for (int s = 0; s < RST_STAGES - 1; ++s) issue(s);
+    for (int64_t q = 0; q < Q; ++q) {
+        issue(q + RST_STAGES - 1);
+        cp_async_wait<RST_STAGES - 1>();
+        __syncwarp();
+        const RstMeta m = meta[q % RST_STAGES];
+        const int L = m.len, p = m.p;
+        if (m.live) {
+            const T* sb = ring + (size_t)(q % RST_STAGES) * WP;
+            if (L != cachedL) {
+                cachedL = L;
+                const int ncand = (L + 63) / 64;
+#pragma unroll
+                for (int h = 0; h < 2; ++h) {
+                    const int c = 2 * lane + h;
+                    lhas[h] = false;
+                    if (c < ncand) {
+                        const int mm = c * 64;
+                        int off = 0, len = L, path = 0, depth = 0;
+                        while (len > PW_BLOCK) {
+                            const int n2 = pw_split32(len);
+                            path <<= 1;
+                            depth++;
+                            if (mm < off + n2) len = n2; else { off += n2; len -= n2; path |= 1; }
+                        }
+                        lhas[h] = off > mm - 64;  // the leaf starts in this candidate window
+                        loff[h] = off;
+                        llen[h] = len;
+                        lsi[h] = path << (Dl - depth);
+                    }
+                }
+            }
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                if (!lhas[h]) continue;
+                const int off = loff[h], len = llen[h];
+                const int lim = len & ~7;
+                A r[8];
+                bool fast = len == PW_BLOCK && (off & (PW_BLOCK - 1)) == 0;
+                if (fast) {
+                    // a whole 128-element leaf in one padded block: 16-byte
+                    // loads, the 8 accumulators as 8 independent chains of
+                    // plain adds; a chain that ends in NaN is replayed with
+                    // the engine's NaN rule below
+                    const T* src = sb + off + PADE * (off >> 7);
+#pragma unroll
+                    for (int j = 0; j < 16; ++j) {
+                        T x[8];
+#pragma unroll
+                        for (int v = 0; v < 8 / VE; ++v) {
+                            uint4 w = *reinterpret_cast<const uint4*>(src + 8 * j + v * VE);
+                            memcpy(&x[v * VE], &w, 16);
+                        }
+#pragma unroll
+                        for (int kk = 0; kk < 8; ++kk) r[kk] = j == 0 ? x[kk] : plain_add(r[kk], x[kk]);
+                    }
+                    bool nan = false;
+#pragma unroll
+                    for (int kk = 0; kk < 8; ++kk) nan |= r[kk] != r[kk];
+                    fast = !nan;
+                }
+                if (!fast) {
+#pragma unroll
+                    for (int kk = 0; kk < 8; ++kk) r[kk] = sb[rst_phys<T>(off + kk)];
+                    for (int j = 8; j < lim; j += 8) {
+#pragma unroll
+                        for (int kk = 0; kk < 8; ++kk) r[kk] = P::fold(r[kk], sb[rst_phys<T>(off + j + kk)]);
+                    }
+                }
+                A res = P::fold(P::fold(P::fold(r[0], r[1]), P::fold(r[2], r[3])), P::fold(P::fold(r[4], r[5]), P::fold(r[6], r[7])));
+                for (int i = lim; i < len; ++i) res = P::fold(res, sb[rst_phys<T>(off + i)]);
+                lslot[lsi[h]] = res;
+                lvalid[lsi[h]] = 1;
+            }
+            __syncwarp();
+            const A wsum = warp_slot_tree<P>(lslot, lvalid, Dl, lane);
+            __syncwarp();
+            lvalid[lane] = 0;
+            lvalid[lane + 32] = 0;
+            if (lane == 0) {
+                uslot[p] = wsum;
+                uvalid[p] = 1;
+            }
+            __syncwarp();
+        }
+        if (p == NW - 1) {  // the segment's last window (live or not)
+            const int64_t u = m.unit;
+            const A r = warp_slot_tree<P>(uslot, uvalid, Dw, lane);
+            __syncwarp();
+            uvalid[lane] = 0;
+            uvalid[lane + 32] = 0;
+            if (lane == 0) {
+                if (d.K == 0) {
+                    int64_t in_off, out_off;
+                    kept_offsets(d, u, &in_off, &out_off);  // K == 0: the unit is the output index
+                    store_cast<CD>(d.o, out_off, d.odt, P::finish(r, d.has_seed, d.seed));
+                } else {
+                    reinterpret_cast<A*>(d.scratch)[u] = r;
+                }
+            }
+            __syncwarp();
+        }
+    }
+    cp_async_wait<0>();
+}
+
+// Order-free accumulator of k_red_rowco: the fold of the non-NaN elements
+// (any order gives the same bits) plus, for floats, the first NaN and its
+// index.
+template <int OP, int CD> struct CoAcc {
+    typedef typename DT<CD>::T T;
+    static constexpr bool FL = dt_is_float(CD);
+    T v;
+    int have;
+    T nanv;
+    int64_t nidx;
+    __device__ __forceinline__ void init() {
+        have = 0;
+        nidx = INT64_MAX;
+        v = T{};
+        nanv = T{};
+    }
+    __device__ __forceinline__ void add(T x, int64_t idx) {
+        if constexpr (FL) {
+            if (x != x) {
+                if (idx < nidx) { nidx = idx; nanv = x; }
+                return;
+            }
+        }
+        v = have ? BinOp<OP, CD>::apply(v, x) : x;
+        have = 1;
+    }
+    __device__ __forceinline__ void merge(const CoAcc& o) {
+        if (o.have) {
+            v = have ? BinOp<OP, CD>::apply(v, o.v) : o.v;
+            have = 1;
+        }
+        if constexpr (FL) {
+            if (o.nidx < nidx) { nidx = o.nidx; nanv = o.nanv; }
+        }
+    }
+    __device__ __forceinline__ void shfl_merge(int h) {
+        CoAcc o;
+        o.v = __shfl_down_sync(0xffffffffu, v, h);
+        o.have = __shfl_down_sync(0xffffffffu, have, h);
+        if constexpr (FL) {
+            o.nanv = __shfl_down_sync(0xffffffffu, nanv, h);
+            o.nidx = __shfl_down_sync(0xffffffffu, nidx, h);
+        } else {
+            o.nidx = INT64_MAX;
+        }
+        merge(o);
+    }
+    // the fold's result: the first NaN if there is one
+    __device__ __forceinline__ T result() const {
+        if constexpr (FL) {
+            if (nidx != INT64_MAX) return nanv;
+        }
+        return v;
+    }
+};
+
+template <int OP, int CD>
+__global__ void __launch_bounds__(RED_THREADS, RCO_CTAS) k_red_rowco(RedDesc d) {
+    typedef typename DT<CD>::T T;
+    typedef CoAcc<OP, CD> C;
+    constexpr int VE = 16 / (int)sizeof(T);
+    constexpr int CH = 32 * VE;  // elements per 512-byte warp chunk
+    constexpr int NWARP = RED_THREADS / 32;
+    __shared__ C wacc[NWARP];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int64_t nseg = (int64_t)1 << d.K;
+    const int64_t nunits = d.nout * nseg;
+    for (int64_t u = blockIdx.x; u < nunits; u += gridDim.x) {
+        int64_t in_off, out_off, soff, slen;
+        kept_offsets(d, u >> d.K, &in_off, &out_off);
+        seg_of(d.w, d.K, u & (nseg - 1), &soff, &slen);
+        const T* base = reinterpret_cast<const T*>(d.a) + in_off + soff;
+        const int64_t nch = (slen + CH - 1) / CH;
+        const int64_t c0 = nch * warp / NWARP, c1 = nch * (warp + 1) / NWARP;
+        C acc;
+        acc.init();
+        // whole chunks, RCO_U in flight; then the rest one at a time (the
+        // segment's last chunk may be partial)
+        const int64_t cfull = c1 < slen / CH ? c1 : (slen / CH > c0 ? slen / CH : c0);
+        int64_t c = c0;
+        for (; c + RCO_U <= cfull; c += RCO_U) {
+            uint4 wv[RCO_U];
+#pragma unroll
+            for (int j = 0; j < RCO_U; ++j) wv[j] = __ldg(reinterpret_cast<const uint4*>(base + (c + j) * CH + lane * VE));
+#pragma unroll
+            for (int j = 0; j < RCO_U; ++j) {
+                T x[VE];
+                memcpy(x, &wv[j], 16);
+                const int64_t e = (c + j) * CH + lane * VE;
+#pragma unroll
+                for (int i = 0; i < VE; ++i) acc.add(x[i], e + i);
+            }
+        }
+        for (; c < c1; ++c) {
+            const int64_t e = c * CH + lane * VE;
+            if (e + VE <= slen) {
+                uint4 wv = __ldg(reinterpret_cast<const uint4*>(base + e));
+                T x[VE];
+                memcpy(x, &wv, 16);
+#pragma unroll
+                for (int i = 0; i < VE; ++i) acc.add(x[i], e + i);
+            } else {
+                for (int64_t i = e; i < slen; ++i) acc.add(base[i], i);
+            }
+        }
+#pragma unroll
+        for (int h = 16; h >= 1; h >>= 1) acc.shfl_merge(h);
+        if (lane == 0) wacc[warp] = acc;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            C r = wacc[0];
+            for (int w = 1; w < NWARP; ++w) r.merge(wacc[w]);
+            const T tot = r.result();
+            if (d.K == 0) {
+                if (d.has_seed) {
+                    T s;
+                    memcpy(&s, &d.seed, sizeof(T));
+                    store_cast<CD>(d.o, out_off, d.odt, BinOp<OP, CD>::apply(s, tot));
+                } else {
+                    store_cast<CD>(d.o, out_off, d.odt, tot);
+                }
+            } else {
+                reinterpret_cast<T*>(d.scratch)[u] = tot;
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// Narrow rows (k_red_rownar): C-contiguous rows of 16..256 bytes (a float64
+// row of 16 elements is 128 bytes). A CTA streams windows of up to 2048 whole
+// rows (32 KiB) into a 3-stage cp.async ring; 16-byte chunk G of a window is
+// stored at G ^ ((G >> 3) & 7), so the 8 lanes that one 16-byte shared load
+// serves, each reading the same chunk of its own row, hit distinct banks.
+// One thread folds one row with the leaf rule of pairwise_sum (8 interleaved
+// accumulators, ufunc.rs:6416-6448) for float add and strictly left to right
+// for every other op; every output is written directly.
+constexpr int NAR_WIN_BYTES = 32768;
+constexpr int NAR_STAGES = 3;
+constexpr int NAR_CTAS = 2;
+constexpr int NAR_MAXROWB = 256;
+__device__ __forceinline__ int nar_swz(int g) { return g ^ ((g >> 3) & 7); }
+
+template <int OP, int CD>
+__global__ void __launch_bounds__(RED_THREADS, NAR_CTAS) k_red_rownar(RedDesc d) {
+    typedef RPol<OP, CD> P;
+    typedef typename P::A A;
+    typedef typename DT<CD>::T T;
+    static_assert(sizeof(A) == sizeof(T), "no widening in the narrow-row kernel");
+    constexpr int VE = 16 / (int)sizeof(T);
+    constexpr bool PW8 = !P::CHUNK && dt_is_float(CD);  // float add: the 8-accumulator leaf
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    uint4* ring = reinterpret_cast<uint4*>(smem_raw);
+    constexpr int WCH = NAR_WIN_BYTES / 16;  // chunks per stage
+    const int w = (int)d.w;
+    const int m = w / VE;  // chunks per row
+    const int R = WCH / m < 2048 ? WCH / m : 2048;
+    const int64_t nwin = (d.nout + R - 1) / R;
+    const int64_t myw = nwin > blockIdx.x ? (nwin - blockIdx.x + gridDim.x - 1) / gridDim.x : 0;
+    const uint4* a = reinterpret_cast<const uint4*>(d.a);
+    auto issue = [&](int64_t q) {
+        if (q < myw) {
+            const int64_t r0 = (blockIdx.x + q * (int64_t)gridDim.x) * R;
+            const int64_t rows = d.nout - r0 < R ? d.nout - r0 : R;
+            const int nch = (int)rows * m;
+            uint4* sb = ring + (size_t)(q % NAR_STAGES) * WCH;
+            const uint4* src = a + r0 * m;
+            for (int c = threadIdx.x; c < nch; c += RED_THREADS) cp_async16(sb + nar_swz(c), src + c);
+        }
+        cp_async_commit();
+    };
+    for (int s = 0; s < NAR_STAGES - 1; ++s) issue(s);
+    for (int64_t q = 0; q < myw; ++q) {
+        issue(q + NAR_STAGES - 1);
+        cp_async_wait<NAR_STAGES - 1>();
+        __syncthreads();
+        const int64_t r0 = (blockIdx.x + q * (int64_t)gridDim.x) * R;
+        const int rows = (int)(d.nout - r0 < R ? d.nout - r0 : R);
+        const uint4* sb = ring + (size_t)(q % NAR_STAGES) * WCH;
+        for (int r = threadIdx.x; r < rows; r += RED_THREADS) {
+            const int g0 = r * m;
+            auto chunk = [&](int c, T (&x)[VE]) {
+                uint4 v = sb[nar_swz(g0 + c)];
+                memcpy(x, &v, 16);
+            };
+            A res;
+            int done;  // elements folded
+            if (PW8 && w >= 8) {
+                A acc[8];
+                const int lim = w & ~7;
+#pragma unroll
+                for (int cc = 0; cc < 8 / VE; ++cc) {
+                    T x[VE];
+                    chunk(cc, x);
+#pragma unroll
+                    for (int i = 0; i < VE; ++i) acc[cc * VE + i] = x[i];
+                }
+                for (int e = 8; e < lim; e += 8) {
+#pragma unroll
+                    for (int cc = 0; cc < 8 / VE; ++cc) {
+                        T x[VE];
+                        chunk(e / VE + cc, x);
+#pragma unroll
+                        for (int i = 0; i < VE; ++i) acc[cc * VE + i] = P::fold(acc[cc * VE + i], x[i]);
+                    }
+                }
+                res = P::fold(P::fold(P::fold(acc[0], acc[1]), P::fold(acc[2], acc[3])),
+                              P::fold(P::fold(acc[4], acc[5]), P::fold(acc[6], acc[7])));
+                done = lim;
+            } else {
+                T x[VE];
+                chunk(0, x);
+                res = x[0];
+#pragma unroll
+                for (int i = 1; i < VE; ++i) res = P::fold(res, x[i]);
+                done = VE;
+            }
+            for (int c = done / VE; c < m; ++c) {  // tail (or the rest of a sequential fold), in order
+                T x[VE];
+                chunk(c, x);
+#pragma unroll
+                for (int i = 0; i < VE; ++i)
+                    if (c * VE + i >= done) res = P::fold(res, x[i]);
+            }
+            store_cast<CD>(d.o, (r0 + r) * d.kost[0], d.odt, P::finish(res, d.has_seed, d.seed));  // one kept dim
+        }
+        __syncthreads();
+    }
+    cp_async_wait<0>();
+}
+
+// ---------------------------------------------------------------------------
+// Host side: which rows take these kernels, and their launch.
+// ---------------------------------------------------------------------------
+constexpr bool rowst_type_ok(int op, int cd) { return op == OP_ADD && (cd == DT_F32 || cd == DT_F64); }
+constexpr bool rowco_type_ok(int op, int cd) {
+    const bool w48 = cd == DT_I32 || cd == DT_I64 || cd == DT_U32 || cd == DT_U64 || cd == DT_F32 || cd == DT_F64;
+    if (!w48) return false;
+    if (op == OP_MAXIMUM || op == OP_MINIMUM) return true;
+    return !dt_is_float(cd) && (op == OP_ADD || op == OP_MULTIPLY || op == OP_BITWISE_AND || op == OP_BITWISE_OR ||
+                                op == OP_BITWISE_XOR);
+}
+
+// Contiguous runs whose every start is 16-byte aligned, long enough to keep a
+// CTA busy per segment.
+inline bool row_wide_ok(const RedDesc& d, int es) {
+    if (d.ws != 1 || d.w < 2048 || d.adt != d.cd) return false;
+    if ((reinterpret_cast<uintptr_t>(d.a) & 15) != 0) return false;
+    for (int i = 0; i < d.nk; ++i)
+        if ((d.kst[i] * es) % 16 != 0) return false;
+    return true;
+}
+
+inline int rst_depth(int64_t n, std::map<int64_t, int>& memo) {
+    if (n <= PW_BLOCK) return 0;
+    auto it = memo.find(n);
+    if (it != memo.end()) return it->second;
+    int64_t n2 = pw_split(n);
+    int dd = 1 + std::max(rst_depth(n2, memo), rst_depth(n - n2, memo));
+    memo[n] = dd;
+    return dd;
+}
+
+// Window depth Dw (all nodes at that depth fit one window) and leaf-slot
+// depth Dl for the segments of run_row's K-level split; false when either
+// slot array would exceed 64 entries.
+inline bool rst_plan(int64_t w, int K, int win, int* Dw, int* Dl) {
+    std::set<int64_t> cur{w};
+    for (int i = 0; i < K; ++i) {
+        std::set<int64_t> nx;
+        for (int64_t l : cur) {
+            int64_t n2 = pw_split(l);
+            nx.insert(n2);
+            nx.insert(l - n2);
+        }
+        cur.swap(nx);
+    }
+    int dw = 0;
+    while (*cur.rbegin() > win) {
+        std::set<int64_t> nx;
+        for (int64_t l : cur) {
+            if (l <= PW_BLOCK) { nx.insert(l); continue; }
+            int64_t n2 = pw_split(l);
+            nx.insert(n2);
+            nx.insert(l - n2);
+        }
+        cur.swap(nx);
+        if (++dw > RST_MAXDW) return false;
+    }
+    std::map<int64_t, int> memo;
+    int dl = 0;
+    for (int64_t l : cur) dl = std::max(dl, rst_depth(l, memo));
+    if (dl > RST_MAXDL) return false;
+    *Dw = dw;
+    *Dl = dl;
+    return true;
+}
+
+// C-contiguous rows of 16..256 bytes, each a whole number of 16-byte chunks.
+inline bool row_narrow_ok(const RedDesc& d, int es) {
+    if (d.ws != 1 || d.adt != d.cd || d.K != 0 || d.nk != 1 || d.kst[0] != d.w) return false;
+    const int64_t rb = d.w * es;
+    if (rb % 16 != 0 || rb < 16 || rb > NAR_MAXROWB) return false;
+    return (reinterpret_cast<uintptr_t>(d.a) & 15) == 0 && d.nout >= 148 * 256;
+}
+constexpr bool rownar_type_ok(int op, int cd) { return rowst_type_ok(op, cd) || rowco_type_ok(op, cd); }
+
+// Launch the wide-row kernel for (OP, CD) if the run qualifies; returns
+// cudaErrorNotSupported (nothing launched) otherwise.
+template <int OP, int CD>
+static cudaError_t launch_row_wide(const RedDesc& din, cudaStream_t s) {
+    typedef typename DT<CD>::T T;
+    if constexpr (rownar_type_ok(OP, CD)) {
+        if (row_narrow_ok(din, (int)sizeof(T))) {
+            const int64_t R = std::min<int64_t>(2048, (NAR_WIN_BYTES / 16) / (din.w * (int64_t)sizeof(T) / 16));
+            const int64_t nwin = (din.nout + R - 1) / R;
+            const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(nwin, 148LL * NAR_CTAS));
+            auto k = k_red_rownar<OP, CD>;
+            const size_t smem = (size_t)NAR_STAGES * NAR_WIN_BYTES;
+            cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+            k<<<grid, RED_THREADS, smem, s>>>(din);
+            count_launch();
+            return cudaGetLastError();
+        }
+    }
+    if constexpr (rowst_type_ok(OP, CD)) {
+        if (!row_wide_ok(din, (int)sizeof(T))) return cudaErrorNotSupported;
+        RedDesc d = din;
+        if (!rst_plan(d.w, d.K, RST_WIN, &d.Dw, &d.Dl)) return cudaErrorNotSupported;
+        const int64_t units = d.nout << d.K;
+        auto k = k_red_rowst<OP, CD>;
+        const size_t smem = rst_smem<T>();
+        cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        int per_sm = 1;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, 32 * rst_warps<T>(), smem);
+        const int64_t ctas = (units + rst_warps<T>() - 1) / rst_warps<T>();
+        const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(ctas, 148LL * std::max(per_sm, 1)));
+        k<<<grid, 32 * rst_warps<T>(), smem, s>>>(d);
+        count_launch();
+        return cudaGetLastError();
+    } else if constexpr (rowco_type_ok(OP, CD)) {
+        if (!row_wide_ok(din, (int)sizeof(T))) return cudaErrorNotSupported;
+        const int64_t units = din.nout << din.K;
+        const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(units, 148LL * RCO_CTAS));
+        k_red_rowco<OP, CD><<<grid, RED_THREADS, 0, s>>>(din);
+        count_launch();
+        return cudaGetLastError();
+    } else {
+        return cudaErrorNotSupported;
+    }
+}
+
+}  // namespace ionp

@@ -40,6 +40,20 @@ template <int OPV>
 static cudaError_t col_op(const RedDesc& d, cudaStream_t s) {
     const bool castld = d.adt != d.cd;
     const int grid = seq_grid(d.nout, RED_THREADS);
+    // fewer than 64K outputs over one long narrow axis of 4- or 8-byte
+    // elements: one thread per output with 64 loads in flight
+    if (!castld && d.nr == 1 && d.nout < 65536 && d.rshape[0] >= 256 && dt_size(d.cd) >= 4) {
+#define IONP_U64CASE(D)                                                                  \
+        case D:                                                                          \
+            if constexpr (red_any_valid(OPV, D) && (sizeof(typename DT<D>::T) >= 4)) {   \
+                k_red_col<OPV, D, false, 64><<<grid, RED_THREADS, 0, s>>>(d);            \
+                count_launch();                                                          \
+                return cudaGetLastError();                                               \
+            }                                                                            \
+            break;
+        switch (d.cd) { IONP_DTS(IONP_U64CASE) }
+#undef IONP_U64CASE
+    }
     if (col_staged_ok(d, dt_size(d.cd))) {
 #define IONP_STCASE(D)                                                                   \
         case D:                                                                          \
@@ -68,6 +82,32 @@ static cudaError_t col_op(const RedDesc& d, cudaStream_t s) {
 
 cudaError_t launch_reduce_col(const RedDesc& d, cudaStream_t s) {
 #define IONP_OPCASE(OP) case OP: return col_op<OP>(d, s);
+    switch (d.op) { IONP_RED_OPS(IONP_OPCASE) }
+#undef IONP_OPCASE
+    return cudaErrorInvalidValue;
+}
+
+template <int OPV>
+static cudaError_t col_split_op(const RedDesc& d, cudaStream_t s) {
+    const int64_t ntask = d.nout << d.K;
+    int64_t g = (ntask + RED_THREADS - 1) / RED_THREADS;
+    if (g > 148 * 8) g = 148 * 8;
+    const int grid = (int)(g < 1 ? 1 : g);
+#define IONP_DTCASE(D)                                                  \
+    case D:                                                             \
+        if constexpr (red_assoc(OPV, D)) {                              \
+            k_red_col_split<OPV, D><<<grid, RED_THREADS, 0, s>>>(d);    \
+            count_launch();                                             \
+            return cudaGetLastError();                                  \
+        }                                                               \
+        break;
+    switch (d.cd) { IONP_DTS(IONP_DTCASE) }
+#undef IONP_DTCASE
+    return cudaErrorInvalidValue;
+}
+
+cudaError_t launch_reduce_col_split(const RedDesc& d, cudaStream_t s) {
+#define IONP_OPCASE(OP) case OP: return col_split_op<OP>(d, s);
     switch (d.op) { IONP_RED_OPS(IONP_OPCASE) }
 #undef IONP_OPCASE
     return cudaErrorInvalidValue;

@@ -1,8 +1,11 @@
 """Autotuner and learned schedule picker for batched calls.
 
 * The **autotuner** times a call under every one of the 48 schedules
-  (``Batch.time_call``: the call run alone as its own queue, CUDA events) and
-  keeps the fastest. It is exact but costs 48 timed runs per call.
+  (``Batch.time_call``: the call queued enough times in one persistent launch
+  to fill the GPU, every copy on its own operand region so that the copies
+  stream from HBM like the distinct calls of a real batch; CUDA events, time
+  per copy) and keeps the fastest. It is exact but costs 48 timed runs per
+  call.
 * The **picker** is a 3-layer perceptron (width 64, FP32; forward, backward
   and Adam are this library's own CUDA kernels, ``ionp_mlp_*``) that maps a
   call's features (``ionp_batch_features``: op class, call kind, operand

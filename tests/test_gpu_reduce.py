@@ -171,3 +171,151 @@ def test_argext_errors():
         ap.argmax(ap.from_numpy(np.zeros(0)))
     with pytest.raises(ap.AxisError):
         ap.argmin(ap.from_numpy(np.zeros((2, 2))), axis=2)
+
+
+WIDE = [((3, 2048), -1), ((2, 4096), 1), ((5, 5000), -1), ((2, 2049), 1), ((3, 65536), -1), ((2, 65544), 1),
+        ((1, 300007), -1), ((2, 200000), -1), ((1 << 21,), 0), ((4, 8, 4096), (1, 2)), ((16, 8192), None)]
+
+
+def _nan_payloads(a, rng, frac):
+    """Scatter NaNs with distinct payloads and signs, so only the first NaN in
+    fold order is the right answer."""
+    flat = a.reshape(-1)
+    pos = np.nonzero(rng.random(flat.size) < frac)[0]
+    if flat.dtype == np.float32:
+        pay = (0x7FC00000 | rng.integers(1, 1 << 22, pos.size)) | (rng.integers(0, 2, pos.size) << 31)
+        flat.view(np.uint32)[pos] = pay.astype(np.uint32)
+    else:
+        pay = (0x7FF8000000000000 | rng.integers(1, 1 << 51, pos.size, dtype=np.int64)).astype(np.uint64)
+        pay |= rng.integers(0, 2, pos.size).astype(np.uint64) << np.uint64(63)
+        flat.view(np.uint64)[pos] = pay
+    return a
+
+
+@pytest.mark.parametrize("shape,axis", WIDE, ids=str)
+@pytest.mark.parametrize("dt", [np.float32, np.float64], ids=lambda d: np.dtype(d).name)
+def test_wide_rows_float(shape, axis, dt):
+    """Contiguous runs of >= 2048 elements (the staged pairwise kernel and the
+    order-free max/min kernel), aligned and unaligned row starts, split runs."""
+    rng = np.random.default_rng(sum(shape))
+    a = (rng.standard_normal(shape) * 50).astype(dt)
+    a.reshape(-1)[rng.random(a.size) < 0.01] = 0.0
+    a.reshape(-1)[rng.random(a.size) < 0.01] = -0.0
+    d = ap.from_numpy(a)
+    check_reduce("add", a, d, axis=axis)
+    check_reduce("add", a, d, axis=axis, initial=1.25, keepdims=True)
+    for op in ("maximum", "minimum"):
+        check_reduce(op, a, d, axis=axis)
+    nan = _nan_payloads(a.copy(), rng, 2e-4)
+    dn = ap.from_numpy(nan)
+    for op in ("maximum", "minimum", "add"):
+        check_reduce(op, nan, dn, axis=axis)
+    # a view whose start is 4 bytes past an aligned address
+    flat = (rng.standard_normal(a.size + 1) * 3).astype(dt)
+    check_reduce("add", flat[1:], ap.from_numpy(flat)[1:], axis=0)
+    check_reduce("maximum", flat[1:], ap.from_numpy(flat)[1:], axis=0)
+
+
+@pytest.mark.parametrize("shape,axis", WIDE, ids=str)
+@pytest.mark.parametrize("dt", [np.int32, np.int64, np.uint32, np.uint64], ids=lambda d: np.dtype(d).name)
+def test_wide_rows_int(shape, axis, dt):
+    rng = np.random.default_rng(7 + sum(shape))
+    a = array(dt, shape, rng)
+    d = ap.from_numpy(a)
+    for op in ("add", "multiply", "maximum", "minimum", "bitwise_and", "bitwise_or", "bitwise_xor"):
+        check_reduce(op, a, d, axis=axis)
+    check_reduce("add", a, d, axis=axis, initial=5, keepdims=True)
+
+
+NARROW = [((40000, 16), np.float64), ((38000, 2), np.float64), ((38000, 6), np.float64), ((40000, 10), np.float64),
+          ((38000, 32), np.float64), ((40000, 4), np.float32), ((40000, 12), np.float32), ((40000, 64), np.float32),
+          ((4, 10000, 16), np.float64), ((40000, 16), np.int64), ((40000, 8), np.int32), ((40000, 20), np.uint32)]
+
+
+@pytest.mark.parametrize("shape,dt", NARROW, ids=str)
+def test_narrow_rows(shape, dt):
+    """Many short C-contiguous rows reduced over the last axis (the staged
+    thread-per-row kernel): leaf rule for float add, in-order folds else."""
+    rng = np.random.default_rng(shape[-1])
+    if np.dtype(dt).kind == "f":
+        a = (rng.standard_normal(shape) * 20).astype(dt)
+        a.reshape(-1)[rng.random(a.size) < 0.01] = -0.0
+        ops = ("add", "maximum", "minimum")
+    else:
+        a = array(dt, shape, rng)
+        ops = ("add", "multiply", "maximum", "minimum", "bitwise_xor")
+    d = ap.from_numpy(a)
+    for op in ops:
+        check_reduce(op, a, d, axis=-1)
+    check_reduce("add", a, d, axis=-1, keepdims=True, initial=3)
+    if np.dtype(dt).kind == "f":
+        nan = _nan_payloads(a.copy(), rng, 0.02)
+        dn = ap.from_numpy(nan)
+        for op in ("maximum", "minimum", "add"):
+            check_reduce(op, nan, dn, axis=-1)
+
+
+@pytest.mark.parametrize("shape", [(4096, 64), (2000, 300), (8192, 5), (1024, 4736)], ids=str)
+@pytest.mark.parametrize("dt", [np.float32, np.float64, np.int32, np.int64, np.uint8, np.bool_], ids=lambda d: np.dtype(d).name)
+def test_axis0_order_free_split(shape, dt):
+    """Order-free folds over a long leading axis with few outputs: the axis
+    is cut into parts folded in order on top."""
+    rng = np.random.default_rng(shape[0] + shape[1])
+    a = array(dt, shape, rng, specials=False)
+    if np.dtype(dt).kind == "f":
+        a = _nan_payloads(a, rng, 1e-3)
+        a.reshape(-1)[rng.random(a.size) < 0.01] = -0.0
+        ops = ("maximum", "minimum")
+    elif dt == np.bool_:
+        ops = ("logical_and", "logical_or", "logical_xor", "maximum")
+    else:
+        ops = ("add", "multiply", "maximum", "minimum", "bitwise_and", "bitwise_or", "bitwise_xor")
+    d = ap.from_numpy(a)
+    for op in ops:
+        check_reduce(op, a, d, axis=0)
+        check_reduce(op, a, d, axis=0, keepdims=True)
+    if dt != np.bool_:
+        check_reduce("maximum", a, d, axis=0, initial=a.reshape(-1)[5])
+
+
+@pytest.mark.parametrize("which", ["argmax", "argmin"])
+@pytest.mark.parametrize("shape,dt,axis", [((4096, 5000), np.float32, 0), ((2048, 4800), np.float64, 0),
+                                           ((40000, 16), np.float64, 1), ((40000, 4), np.float32, -1),
+                                           ((40000, 8), np.int16, 1), ((38000, 32), np.int64, 1),
+                                           ((4, 10000, 16), np.float64, 2), ((1 << 21,), np.float32, 0),
+                                           ((1 << 19,), np.int64, 0)], ids=str)
+def test_argext_split_and_narrow(which, shape, dt, axis):
+    """Split column scans, the many-short-rows kernel and wide split scans,
+    with ties and NaNs."""
+    rng = np.random.default_rng(len(shape) + shape[-1])
+    if np.dtype(dt).kind == "f":
+        a = np.round(rng.standard_normal(shape) * 4).astype(dt)  # many ties
+        a = _nan_payloads(a, rng, 1e-4)
+    else:
+        a = rng.integers(-3, 4, shape).astype(dt)
+    d = ap.from_numpy(a)
+    for kd in (False, True):
+        want = O.argext(which, a, axis=axis, keepdims=kd)
+        got = getattr(ap, which)(d, axis=axis, keepdims=kd)
+        assert_bits_equal(to_host(got), np.asarray(want), f"{which} {a.dtype}{shape} axis={axis} keepdims={kd}")
+
+
+@pytest.mark.parametrize("shape", [(4096, 64), (512, 70000), (300, 1000)], ids=str)
+@pytest.mark.parametrize("dt", [np.float32, np.float64], ids=lambda d: np.dtype(d).name)
+def test_axis0_float_add_nan_payloads(shape, dt):
+    """Sequential column sums with NaNs of distinct payloads, signaling NaNs
+    (quieted by the first add) and infinities of both signs (inf - inf makes
+    the default NaN): the plain-add fast path must fall back exactly."""
+    rng = np.random.default_rng(shape[1])
+    a = (rng.standard_normal(shape) * 10).astype(dt)
+    a = _nan_payloads(a, rng, 2e-4)
+    ib = np.uint32 if dt == np.float32 else np.uint64
+    snan = np.array([0x7FA00001 if dt == np.float32 else 0x7FF4000000000001], ib).view(dt)[0]
+    a[0, ::7] = snan
+    a[shape[0] // 2, 3::11] = snan
+    a[5, 1::13] = np.inf
+    a[9, 1::13] = -np.inf
+    d = ap.from_numpy(a)
+    check_reduce("add", a, d, axis=0)
+    check_reduce("add", a, d, axis=0, initial=0.5)
+    check_reduce("add", a, d, axis=0, keepdims=True)
