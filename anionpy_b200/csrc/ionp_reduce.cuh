@@ -422,6 +422,24 @@ __global__ void __launch_bounds__(RED_THREADS) k_red_row_top(RedDesc d) {
     }
 }
 
+// Top of a split with few parts of an order-free fold: one thread per
+// output folds its 2^K partials left to right (equal to the tree for these
+// ops) and applies the seed.
+template <int OP, int CD>
+__global__ void __launch_bounds__(RED_THREADS) k_red_row_top_small(RedDesc d) {
+    typedef RPol<OP, CD> P;
+    typedef typename P::A A;
+    const int64_t nseg = (int64_t)1 << d.K;
+    for (int64_t o = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; o < d.nout; o += (int64_t)gridDim.x * blockDim.x) {
+        const A* part = reinterpret_cast<const A*>(d.scratch) + o * nseg;
+        A v = part[0];
+        for (int64_t s = 1; s < nseg; ++s) v = P::fold(v, part[s]);
+        int64_t in_off, out_off;
+        kept_offsets(d, o, &in_off, &out_off);
+        store_cast<CD>(d.o, out_off, d.odt, P::finish(v, d.has_seed, d.seed));
+    }
+}
+
 // COL kernel: sequential fold per output over the narrow dims (fold order),
 // U loads in flight per thread (64 when the outputs are too few for 16 to
 // keep HBM busy).
@@ -961,7 +979,58 @@ __global__ void __launch_bounds__(RED_THREADS) k_argext(RedDesc d) {
         if (!live) hi = lo;
         T best{};
         int64_t bi = -1;
-        if (d.nr == 1) {
+        constexpr int VE = 16 / (int)sizeof(T);
+        const T* pc = (const T*)d.a + base;
+        if (d.nr == 1 && d.rst[0] == 1 && VE > 1 && hi - lo >= (int64_t)VE * TPR &&
+            ((reinterpret_cast<uintptr_t>(pc + lo)) & 15) == 0) {
+            // contiguous: 16-byte vectors (thread t takes vectors t, t+TPR,
+            // ... then the tail element lo + nv*VE + t), so each thread's
+            // elements still come in increasing order; a vector without NaN
+            // against a non-NaN best only needs "strictly greater"
+            const int64_t nv = (hi - lo) / VE;
+            constexpr int UV = 4;
+            int64_t v = t;
+            auto take = [&](const T (&x)[VE], int64_t e0) {
+                bool nan = false;
+                if constexpr (dt_is_float(CD)) {
+#pragma unroll
+                    for (int k = 0; k < VE; ++k) nan |= P::is_nan(x[k]);
+                    nan |= bi >= 0 && P::is_nan(best);
+                }
+                if (bi >= 0 && !nan) {
+#pragma unroll
+                    for (int k = 0; k < VE; ++k) {
+                        const bool c = MAX ? (x[k] > best) : (x[k] < best);
+                        if (c) { best = x[k]; bi = e0 + k; }
+                    }
+                } else {
+#pragma unroll
+                    for (int k = 0; k < VE; ++k)
+                        if (bi < 0 || P::better(x[k], best)) { best = x[k]; bi = e0 + k; }
+                }
+            };
+            for (; v + (int64_t)(UV - 1) * TPR < nv; v += (int64_t)UV * TPR) {
+                uint4 w[UV];
+#pragma unroll
+                for (int u = 0; u < UV; ++u) w[u] = __ldg(reinterpret_cast<const uint4*>(pc + lo + (v + (int64_t)u * TPR) * VE));
+#pragma unroll
+                for (int u = 0; u < UV; ++u) {
+                    T x[VE];
+                    memcpy(x, &w[u], 16);
+                    take(x, lo + (v + (int64_t)u * TPR) * VE);
+                }
+            }
+            for (; v < nv; v += TPR) {
+                uint4 w = __ldg(reinterpret_cast<const uint4*>(pc + lo + v * VE));
+                T x[VE];
+                memcpy(x, &w, 16);
+                take(x, lo + v * VE);
+            }
+            for (int64_t i = lo + nv * VE + t; i < hi; i += TPR) {
+                const T x = pc[i];
+                if (bi < 0 || P::better(x, best)) { best = x; bi = i; }
+            }
+        } else if (d.nr == 1) {
             // one strided run: no index arithmetic per element, eight loads
             // in flight per thread, each thread's elements in increasing order
             const T* p = (const T*)d.a + base;

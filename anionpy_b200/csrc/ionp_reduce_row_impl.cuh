@@ -30,6 +30,15 @@ static cudaError_t row_t2(const RedDesc& d, int tpr, size_t smem, int grid, cuda
 template <int OP, int CD>
 static cudaError_t row_top_t(const RedDesc& d, cudaStream_t s) {
     typedef typename RPol<OP, CD>::A A;
+    if constexpr (red_assoc(OP, CD)) {
+        if (d.K <= 6 && d.nout >= 148 * 8) {
+            int64_t g = (d.nout + RED_THREADS - 1) / RED_THREADS;
+            if (g > 148 * 16) g = 148 * 16;
+            k_red_row_top_small<OP, CD><<<(int)g, RED_THREADS, 0, s>>>(d);
+            count_launch();
+            return cudaGetLastError();
+        }
+    }
     size_t smem = ((size_t)1 << d.K) * sizeof(A);
     int grid = (int)(d.nout < 148 * 8 ? d.nout : 148 * 8);
     auto k = k_red_row_top<OP, CD>;

@@ -38,13 +38,15 @@
 #include "ionp_reduce.cuh"
 
 #include <algorithm>
+#include <climits>
+#include <type_traits>
 #include <map>
 #include <set>
 
 namespace ionp {
 
 constexpr int RST_WIN = 4096;         // elements per window (a subtree of the split tree)
-constexpr int RST_STAGES = 2;         // per-warp ring depth
+constexpr int RST_STAGES = 2;         // per-warp ring depth: one window in flight while one is summed
 constexpr int RST_MAXDW = 6;          // at most 64 windows per segment
 constexpr int RST_MAXDL = 6;          // at most 64 leaves per window (two per lane)
 constexpr int RCO_CTAS = 5;
@@ -160,33 +162,54 @@ __global__ void __launch_bounds__(32 * rst_warps<typename DT<CD>::T>()) k_red_ro
     for (int i = lane; i < 64; i += 32) { uvalid[i] = 0; lvalid[i] = 0; }
     const T* a = reinterpret_cast<const T*>(d.a);
 
-    // the segment of the unit last issued (cached across its windows)
-    int64_t cu = -1, cbase = 0, clen = 0;
+    // the unit last issued: its base, and its windows' nodes (lane l holds
+    // windows l and l + 32)
+    int64_t cu = -1, cbase = 0;
+    int64_t toff[2] = {0, 0};
+    int tlen[2] = {0, 0};
     auto issue = [&](int64_t q) {
         if (q < Q) {
             const int64_t u = gw + (q >> Dw) * GW;
             const int p = (int)(q & (NW - 1));
             if (u != cu) {
-                int64_t in_off, out_off, soff;
+                int64_t in_off, out_off, soff, slen;
                 kept_offsets(d, u >> d.K, &in_off, &out_off);
-                seg_of(d.w, d.K, u & (nseg - 1), &soff, &clen);
+                seg_of(d.w, d.K, u & (nseg - 1), &soff, &slen);
                 cbase = in_off + soff;
                 cu = u;
+#pragma unroll
+                for (int h = 0; h < 2; ++h) {
+                    const int pp = lane + 32 * h;
+                    tlen[h] = -1;
+                    if (pp < NW && !rst_node(slen, Dw, pp, &toff[h], &tlen[h])) tlen[h] = -1;
+                }
             }
-            int64_t noff = 0;
-            int nlen = 0;
-            const bool live = rst_node(clen, Dw, p, &noff, &nlen);
+            const int hsel = p >> 5;
+            const int64_t noff = __shfl_sync(0xffffffffu, hsel ? toff[1] : toff[0], p & 31);
+            const int nlen = __shfl_sync(0xffffffffu, hsel ? tlen[1] : tlen[0], p & 31);
+            const bool live = nlen >= 0;
             if (live) {
                 T* sb = ring + (size_t)(q % RST_STAGES) * WP;
                 const T* src = a + cbase + noff;
-                const int nch = nlen / VE;
-                for (int c = lane; c < nch; c += 32) cp_async16(sb + rst_phys<T>(c * VE), src + c * VE);
-                for (int e = nch * VE + lane; e < nlen; e += 32) cp_async_elem(sb + rst_phys<T>(e), src + e);
+                if (nlen == RST_WIN) {
+                    // a full window: chunk lane + 32 i holds elements
+                    // 128 i / VE ... of block (lane * VE) / 128 + ..., so both
+                    // addresses advance by a constant per i
+#pragma unroll
+                    for (int i = 0; i < RST_WIN / (32 * VE); ++i) {
+                        const int e = (lane + 32 * i) * VE;
+                        cp_async16(sb + e + PADE * (e >> 7), src + e);
+                    }
+                } else {
+                    const int nch = nlen / VE;
+                    for (int c = lane; c < nch; c += 32) cp_async16(sb + rst_phys<T>(c * VE), src + c * VE);
+                    for (int e = nch * VE + lane; e < nlen; e += 32) cp_async_elem(sb + rst_phys<T>(e), src + e);
+                }
             }
             if (lane == 0) {
                 RstMeta& m = meta[q % RST_STAGES];
                 m.unit = u;
-                m.len = nlen;
+                m.len = live ? nlen : 0;
                 m.p = p;
                 m.live = live;
             }
@@ -197,7 +220,7 @@ __global__ void __launch_bounds__(32 * rst_warps<typename DT<CD>::T>()) k_red_ro
     // and 2*lane + 1, 64 elements apart) for the current window length: one
     // 128-element leaf per lane in a regular window
     int cachedL = -1;
-    int loff[2], llen[2], lsi[2];
+    int loff[2] = {0, 0}, llen[2] = {0, 0}, lsi[2] = {0, 0};
     bool lhas[2];
     for (int s = 0; s < RST_STAGES - 1; ++s) issue(s);
     for (int64_t q = 0; q < Q; ++q) {
@@ -231,19 +254,23 @@ __global__ void __launch_bounds__(32 * rst_warps<typename DT<CD>::T>()) k_red_ro
                     }
                 }
             }
+            // a full power-of-two window: lane l sums leaf l, whose slot is l
+            const bool regular = L == RST_WIN && Dl == 5;
+            A mine = A{};
+            bool mine_set = false;
+            // each lane sums its leaves with plain adds, 8 independent
+            // accumulator chains; leaves whose sum is NaN are queued and
+            // then summed again with the engine's NaN rule, 8 lanes per
+            // leaf, so one NaN does not hold the whole warp in a serial
+            // replay
 #pragma unroll
             for (int h = 0; h < 2; ++h) {
-                if (!lhas[h]) continue;
                 const int off = loff[h], len = llen[h];
-                const int lim = len & ~7;
-                A r[8];
-                bool fast = len == PW_BLOCK && (off & (PW_BLOCK - 1)) == 0;
+                const bool fast = lhas[h] && len == PW_BLOCK && (off & (PW_BLOCK - 1)) == 0;
+                bool redo = lhas[h] && !fast;
                 if (fast) {
-                    // a whole 128-element leaf in one padded block: 16-byte
-                    // loads, the 8 accumulators as 8 independent chains of
-                    // plain adds; a chain that ends in NaN is replayed with
-                    // the engine's NaN rule below
                     const T* src = sb + off + PADE * (off >> 7);
+                    A r[8];
 #pragma unroll
                     for (int j = 0; j < 16; ++j) {
                         T x[8];
@@ -255,26 +282,73 @@ __global__ void __launch_bounds__(32 * rst_warps<typename DT<CD>::T>()) k_red_ro
 #pragma unroll
                         for (int kk = 0; kk < 8; ++kk) r[kk] = j == 0 ? x[kk] : plain_add(r[kk], x[kk]);
                     }
-                    bool nan = false;
-#pragma unroll
-                    for (int kk = 0; kk < 8; ++kk) nan |= r[kk] != r[kk];
-                    fast = !nan;
-                }
-                if (!fast) {
-#pragma unroll
-                    for (int kk = 0; kk < 8; ++kk) r[kk] = sb[rst_phys<T>(off + kk)];
-                    for (int j = 8; j < lim; j += 8) {
-#pragma unroll
-                        for (int kk = 0; kk < 8; ++kk) r[kk] = P::fold(r[kk], sb[rst_phys<T>(off + j + kk)]);
+                    const A res = plain_add(plain_add(plain_add(r[0], r[1]), plain_add(r[2], r[3])),
+                                            plain_add(plain_add(r[4], r[5]), plain_add(r[6], r[7])));
+                    if (res == res) {
+                        if (regular) {
+                            mine = res;
+                            mine_set = true;
+                        } else {
+                            lslot[lsi[h]] = res;
+                            lvalid[lsi[h]] = 1;
+                        }
+                    } else {
+                        redo = true;
                     }
                 }
-                A res = P::fold(P::fold(P::fold(r[0], r[1]), P::fold(r[2], r[3])), P::fold(P::fold(r[4], r[5]), P::fold(r[6], r[7])));
-                for (int i = lim; i < len; ++i) res = P::fold(res, sb[rst_phys<T>(off + i)]);
-                lslot[lsi[h]] = res;
-                lvalid[lsi[h]] = 1;
+                unsigned q_mask = __ballot_sync(0xffffffffu, redo);
+                while (q_mask) {
+                    // up to 4 queued leaves at a time, one per 8-lane group
+                    const int gq = lane >> 3, k = lane & 7;
+                    unsigned mm = q_mask;
+                    for (int i = 0; i < gq && mm; ++i) mm &= mm - 1;
+                    const int src_lane = mm ? __ffs(mm) - 1 : 0;
+                    const bool act = mm != 0;
+                    const int qoff = __shfl_sync(0xffffffffu, off, src_lane);
+                    const int qlen = __shfl_sync(0xffffffffu, len, src_lane);
+                    const int qsi = __shfl_sync(0xffffffffu, lsi[h], src_lane);
+                    for (int i = 0; i < 4 && q_mask; ++i) q_mask &= q_mask - 1;
+                    if (act) {
+                        const int lim = qlen & ~7;
+                        const unsigned gm = 0xFFu << (lane & 24);
+                        if (qlen >= 8) {
+                            A r = sb[rst_phys<T>(qoff + k)];
+                            for (int j = 8; j < lim; j += 8) r = P::fold(r, sb[rst_phys<T>(qoff + k + j)]);
+                            A v = __shfl_xor_sync(gm, r, 1);
+                            r = (k & 1) ? P::fold(v, r) : P::fold(r, v);
+                            v = __shfl_xor_sync(gm, r, 2);
+                            r = (k & 2) ? P::fold(v, r) : P::fold(r, v);
+                            v = __shfl_xor_sync(gm, r, 4);
+                            r = (k & 4) ? P::fold(v, r) : P::fold(r, v);
+                            if (k == 0) {
+                                for (int i = lim; i < qlen; ++i) r = P::fold(r, sb[rst_phys<T>(qoff + i)]);
+                                lslot[qsi] = r;
+                                lvalid[qsi] = 1;
+                            }
+                        } else if (k == 0) {  // a leaf of fewer than 8 elements folds in order
+                            A r = sb[rst_phys<T>(qoff)];
+                            for (int i = 1; i < qlen; ++i) r = P::fold(r, sb[rst_phys<T>(qoff + i)]);
+                            lslot[qsi] = r;
+                            lvalid[qsi] = 1;
+                        }
+                    }
+                }
             }
             __syncwarp();
-            const A wsum = warp_slot_tree<P>(lslot, lvalid, Dl, lane);
+            A wsum;
+            if (regular) {
+                // the 32 leaf sums of a perfect tree, folded across lanes
+                // left operand first
+                if (!mine_set) mine = lslot[lane];
+#pragma unroll
+                for (int hh = 1; hh < 32; hh <<= 1) {
+                    const A o = __shfl_down_sync(0xffffffffu, mine, hh);
+                    if ((lane & (2 * hh - 1)) == 0) mine = P::fold(mine, o);
+                }
+                wsum = mine;
+            } else {
+                wsum = warp_slot_tree<P>(lslot, lvalid, Dl, lane);
+            }
             __syncwarp();
             lvalid[lane] = 0;
             lvalid[lane + 32] = 0;
@@ -305,57 +379,121 @@ __global__ void __launch_bounds__(32 * rst_warps<typename DT<CD>::T>()) k_red_ro
     cp_async_wait<0>();
 }
 
-// Order-free accumulator of k_red_rowco: the fold of the non-NaN elements
-// (any order gives the same bits) plus, for floats, the first NaN and its
-// index.
+// Order-free accumulator of k_red_rowco.
+//  * integers: the running fold, started from the op's identity (0 for add,
+//    or and xor, 1 for multiply, all ones for and, the extreme value for
+//    max/min), so every element costs one operation;
+//  * float max/min: the non-NaN elements compared as ordered integer keys
+//    (the bits with the magnitude flipped for negatives, so -0 < +0 and a
+//    maximum tie picks +0 as float_max does), plus the first NaN and its
+//    index; a 16-byte vector without NaN costs one integer max per element.
+template <int CD> struct FKey {
+    typedef typename DT<CD>::T T;
+    typedef typename std::conditional<sizeof(T) == 8, long long, int>::type K;
+    static __device__ __forceinline__ K key(T x) {
+        K b;
+        memcpy(&b, &x, sizeof(T));
+        constexpr int SH = 8 * (int)sizeof(T) - 1;
+        const K mag = (K)(~((unsigned long long)1 << SH) & (sizeof(T) == 8 ? ~0ull : 0xFFFFFFFFull));
+        return b ^ ((b >> SH) & mag);
+    }
+    static __device__ __forceinline__ T val(K k) {
+        const K b = key_inv(k);
+        T x;
+        memcpy(&x, &b, sizeof(T));
+        return x;
+    }
+    static __device__ __forceinline__ K key_inv(K k) {
+        constexpr int SH = 8 * (int)sizeof(T) - 1;
+        const K mag = (K)(~((unsigned long long)1 << SH) & (sizeof(T) == 8 ? ~0ull : 0xFFFFFFFFull));
+        return k ^ ((k >> SH) & mag);
+    }
+};
+
+template <int OP, int CD> struct IntIdentity {
+    typedef typename DT<CD>::T T;
+    static __device__ __forceinline__ T get() {
+        if constexpr (OP == OP_MULTIPLY) return (T)1;
+        else if constexpr (OP == OP_BITWISE_AND) return (T)~(T)0;
+        else if constexpr (OP == OP_MAXIMUM) return dt_is_sint(CD) ? (T)(1ull << (8 * sizeof(T) - 1)) : (T)0;
+        else if constexpr (OP == OP_MINIMUM) return dt_is_sint(CD) ? (T)~(1ull << (8 * sizeof(T) - 1)) : (T)~(T)0;
+        else return (T)0;
+    }
+};
+
 template <int OP, int CD> struct CoAcc {
     typedef typename DT<CD>::T T;
     static constexpr bool FL = dt_is_float(CD);
-    T v;
-    int have;
+    static constexpr bool MX = OP == OP_MAXIMUM;
+    typedef typename FKey<CD>::K K;
+    T v;        // integers: the fold so far
+    K kv;       // floats: best key so far (sentinel: nothing yet)
     T nanv;
     int64_t nidx;
-    __device__ __forceinline__ void init() {
-        have = 0;
-        nidx = INT64_MAX;
-        v = T{};
-        nanv = T{};
+    static __device__ __forceinline__ K none() {
+        if constexpr (sizeof(T) == 8) return MX ? (K)LLONG_MIN : (K)LLONG_MAX;
+        else return MX ? (K)INT_MIN : (K)INT_MAX;
     }
+    __device__ __forceinline__ void init() {
+        nidx = INT64_MAX;
+        nanv = T{};
+        if constexpr (FL) kv = none();
+        else v = IntIdentity<OP, CD>::get();
+    }
+    __device__ __forceinline__ void addk(K k) { kv = MX ? (k > kv ? k : kv) : (k < kv ? k : kv); }
     __device__ __forceinline__ void add(T x, int64_t idx) {
         if constexpr (FL) {
             if (x != x) {
                 if (idx < nidx) { nidx = idx; nanv = x; }
                 return;
             }
+            addk(FKey<CD>::key(x));
+        } else {
+            v = BinOp<OP, CD>::apply(v, x);
         }
-        v = have ? BinOp<OP, CD>::apply(v, x) : x;
-        have = 1;
+    }
+    template <int VE> __device__ __forceinline__ void add_vec(const T (&x)[VE], int64_t e0) {
+        if constexpr (FL) {
+            bool nan = false;
+#pragma unroll
+            for (int i = 0; i < VE; ++i) nan |= x[i] != x[i];
+            if (!nan) {
+#pragma unroll
+                for (int i = 0; i < VE; ++i) addk(FKey<CD>::key(x[i]));
+            } else {
+#pragma unroll
+                for (int i = 0; i < VE; ++i) add(x[i], e0 + i);
+            }
+        } else {
+#pragma unroll
+            for (int i = 0; i < VE; ++i) v = BinOp<OP, CD>::apply(v, x[i]);
+        }
     }
     __device__ __forceinline__ void merge(const CoAcc& o) {
-        if (o.have) {
-            v = have ? BinOp<OP, CD>::apply(v, o.v) : o.v;
-            have = 1;
-        }
         if constexpr (FL) {
+            addk(o.kv);
             if (o.nidx < nidx) { nidx = o.nidx; nanv = o.nanv; }
+        } else {
+            v = BinOp<OP, CD>::apply(v, o.v);
         }
     }
     __device__ __forceinline__ void shfl_merge(int h) {
         CoAcc o;
-        o.v = __shfl_down_sync(0xffffffffu, v, h);
-        o.have = __shfl_down_sync(0xffffffffu, have, h);
         if constexpr (FL) {
+            o.kv = __shfl_down_sync(0xffffffffu, kv, h);
             o.nanv = __shfl_down_sync(0xffffffffu, nanv, h);
             o.nidx = __shfl_down_sync(0xffffffffu, nidx, h);
         } else {
-            o.nidx = INT64_MAX;
+            o.v = __shfl_down_sync(0xffffffffu, v, h);
         }
         merge(o);
     }
-    // the fold's result: the first NaN if there is one
+    // the fold's result: the first NaN if there is one (every segment has
+    // at least one element, so a float fold without NaN has a key)
     __device__ __forceinline__ T result() const {
         if constexpr (FL) {
             if (nidx != INT64_MAX) return nanv;
+            return FKey<CD>::val(kv);
         }
         return v;
     }
@@ -393,9 +531,7 @@ __global__ void __launch_bounds__(RED_THREADS, RCO_CTAS) k_red_rowco(RedDesc d) 
             for (int j = 0; j < RCO_U; ++j) {
                 T x[VE];
                 memcpy(x, &wv[j], 16);
-                const int64_t e = (c + j) * CH + lane * VE;
-#pragma unroll
-                for (int i = 0; i < VE; ++i) acc.add(x[i], e + i);
+                acc.template add_vec<VE>(x, (c + j) * CH + lane * VE);
             }
         }
         for (; c < c1; ++c) {
@@ -404,8 +540,7 @@ __global__ void __launch_bounds__(RED_THREADS, RCO_CTAS) k_red_rowco(RedDesc d) 
                 uint4 wv = __ldg(reinterpret_cast<const uint4*>(base + e));
                 T x[VE];
                 memcpy(x, &wv, 16);
-#pragma unroll
-                for (int i = 0; i < VE; ++i) acc.add(x[i], e + i);
+                acc.template add_vec<VE>(x, e);
             } else {
                 for (int64_t i = e; i < slen; ++i) acc.add(base[i], i);
             }

@@ -384,6 +384,27 @@ template <int D> __device__ __forceinline__ typename FOps<D>::T float_floor_divi
     if (O::isinf_(x) && O::isfin(y) && !O::iszero(y)) return O::nan();
     if (O::isinf_(y) && O::isfin(x) && !O::iszero(x) && O::neg(x) != O::neg(y)) return O::negone();
     if (O::isfin(x) && O::isfin(y) && !O::iszero(y)) {
+        if constexpr (D == DT_F32 || D == DT_F64) {
+            // One division: with t = trunc(fl(x / y)) below 2^20 (2^49),
+            // x - t*y is exact in one FMA, one repair step makes t the exact
+            // truncated quotient q and r = fmod(x, y), and npy_divmod's
+            // (x - r) / y then lies within 1/4 of q, so its floor-and-round
+            // gives q (q - 1 after the sign fix) exactly; a zero result takes
+            // npy_divmod's copysign(0, x / y), the sign of x XOR y.
+            const T t = trunc(O::div(x, y));
+            if (fabs(t) < (D == DT_F32 ? (T)0x1p20 : (T)0x1p49)) {
+                T r, q = t;
+                if constexpr (D == DT_F32) r = __fmaf_rn(-t, y, x);
+                else r = __fma_rn(-t, y, x);
+                if (!O::iszero(r) && O::neg(r) != O::neg(x)) {
+                    r = O::add(r, copysign(y, x));
+                    q = O::sub(q, O::neg(x) == O::neg(y) ? (T)1 : (T)-1);
+                }
+                if (!O::iszero(r) && O::neg(r) != O::neg(y)) q = O::sub(q, (T)1);
+                if (q == (T)0) return (O::neg(x) != O::neg(y)) ? (T)-0.0 : (T)0.0;
+                return q;
+            }
+        }
         T raw_r = O::rem(x, y);
         T div = O::div(O::sub(x, raw_r), y);
         if (!O::iszero(raw_r) && O::neg(raw_r) != O::neg(y)) div = O::sub(div, O::one());

@@ -238,3 +238,24 @@ def test_scalar_operands_and_0d():
     assert r.dtype == np.int8
     s = ap.add(ap.from_numpy(np.array(2.5)), ap.from_numpy(np.array(1.0)))
     assert isinstance(s, np.float64) and s == 3.5
+
+
+@pytest.mark.parametrize("dt", [np.float32, np.float64], ids=lambda d: np.dtype(d).name)
+def test_float_floor_divide_quotient_edges(dt):
+    """floor_divide at the edges of the one-division path: quotients just
+    below and above 2^20 (float32) / 2^49 (float64), quotients a rounding
+    away from an integer, exact multiples, zeros of both signs and huge
+    quotients, against the oracle's npy_divmod sequence bit for bit."""
+    rng = np.random.default_rng(77)
+    lim = 2.0 ** 20 if dt == np.float32 else 2.0 ** 49
+    eps = 2.0 ** -23 if dt == np.float32 else 2.0 ** -52
+    n = 40000
+    y = rng.standard_normal(n) * np.exp2(rng.integers(-20, 20, n))
+    q = np.concatenate([rng.integers(1, 64, n // 4), rng.integers(lim // 2, lim * 2, n // 4).astype(np.float64),
+                        rng.integers(1, 1 << 16, n // 4), np.zeros(n - 3 * (n // 4))])
+    x = q * y * (1 + rng.choice([-1.0, 0.0, 1.0], n) * eps) * rng.choice([-1.0, 1.0], n)
+    x[-100:] = rng.choice([0.0, -0.0], 100)
+    xs, ys = x.astype(dt), y.astype(dt)
+    got = ap.floor_divide(ap.from_numpy(xs), ap.from_numpy(ys)).get()
+    want, _ = O.binary("floor_divide", xs, ys)
+    assert_bits_equal(got, want, f"floor_divide {np.dtype(dt).name} quotient edges")
