@@ -997,7 +997,7 @@ __global__ void __launch_bounds__(RED_THREADS) k_argext(RedDesc d) {
                     for (int k = 0; k < VE; ++k) nan |= P::is_nan(x[k]);
                     nan |= bi >= 0 && P::is_nan(best);
                 }
-                if (bi >= 0 && !nan) {
+                if (CD != DT_F16 && bi >= 0 && !nan) {
 #pragma unroll
                     for (int k = 0; k < VE; ++k) {
                         const bool c = MAX ? (x[k] > best) : (x[k] < best);
@@ -1158,8 +1158,22 @@ __global__ void __launch_bounds__(RED_THREADS) k_argext_col(RedDesc d) {
             T x[U];
 #pragma unroll
             for (int u = 0; u < U; ++u) x[u] = p[(i + u) * d.ws];
+            bool nan = false;
+            if constexpr (dt_is_float(CD)) {
 #pragma unroll
-            for (int u = 0; u < U; ++u) if (P::better(x[u], best)) { best = x[u]; bi = i + u; }
+                for (int u = 0; u < U; ++u) nan |= P::is_nan(x[u]);
+                nan |= P::is_nan(best);
+            }
+            if (CD != DT_F16 && !nan) {
+                // no NaN on either side: "better" is a strict comparison
+                // (float16 compares through float in P::better)
+#pragma unroll
+                for (int u = 0; u < U; ++u)
+                    if (MAX ? (x[u] > best) : (x[u] < best)) { best = x[u]; bi = i + u; }
+            } else {
+#pragma unroll
+                for (int u = 0; u < U; ++u) if (P::better(x[u], best)) { best = x[u]; bi = i + u; }
+            }
         }
         for (; i < r1; ++i) {
             T x = p[i * d.ws];

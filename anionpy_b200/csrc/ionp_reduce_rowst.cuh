@@ -48,14 +48,15 @@ namespace ionp {
 constexpr int RST_WIN = 4096;         // elements per window (a subtree of the split tree)
 constexpr int RST_STAGES = 2;         // per-warp ring depth: one window in flight while one is summed
 constexpr int RST_MAXDW = 6;          // at most 64 windows per segment
-constexpr int RST_MAXDL = 6;          // at most 64 leaves per window (two per lane)
+constexpr int RST_MAXDL = 7;          // at most 128 leaves per window (four per lane)
 constexpr int RCO_CTAS = 5;
 constexpr int RCO_U = 4;              // 512-byte chunks in flight per warp
 
 // 16 bytes of padding after every 128 elements: one lane per 128-element
 // leaf, so the lanes of a 16-byte shared load sit 4 banks apart
 template <class T> constexpr int rst_pad() { return 16 / (int)sizeof(T); }
-template <class T> constexpr int rst_win_phys() { return RST_WIN + rst_pad<T>() * (RST_WIN / 128); }
+template <class T> constexpr int rst_win() { return RST_WIN; }
+template <class T> constexpr int rst_win_phys() { return rst_win<T>() + rst_pad<T>() * (rst_win<T>() / 128); }
 template <class T> constexpr int rst_warps() { return sizeof(T) == 4 ? 2 : 1; }  // warps per CTA
 // window element e sits at e + pad * (e / 128) in the stage buffer
 template <class T> __device__ __forceinline__ int rst_phys(int e) { return e + rst_pad<T>() * (e >> 7); }
@@ -90,19 +91,27 @@ template <class T> __device__ __forceinline__ void cp_async_elem(T* smem, const 
     else asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(sa), "l"(gmem) : "memory");
 }
 
-// Warp 0 folds a perfect-binary-tree slot array of 2^D <= 64 entries (lane l
-// holds slots 2l and 2l+1); the root lands in lane 0. A right subtree exists
+// A warp folds a perfect-binary-tree slot array of 2^D <= 128 entries (lane
+// l holds slots 4l..4l+3); the root lands in lane 0. A right subtree exists
 // only where its left sibling does, so a missing right operand leaves the
 // left one unchanged.
 template <class P>
 __device__ __forceinline__ typename P::A warp_slot_tree(const typename P::A* s, const uint8_t* v, int D, int lane) {
     typedef typename P::A A;
     const int ns = 1 << D;
-    const int i0 = 2 * lane, i1 = i0 + 1;
-    A a{};
-    int va = 0;
-    if (i0 < ns && v[i0]) { a = s[i0]; va = 1; }
-    if (i1 < ns && v[i1]) a = P::fold(a, s[i1]);
+    A x[4];
+    int vx[4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        const int j = 4 * lane + i;
+        vx[i] = j < ns && v[j];
+        x[i] = vx[i] ? s[j] : A{};
+    }
+    if (vx[1]) x[0] = P::fold(x[0], x[1]);
+    if (vx[3]) x[2] = P::fold(x[2], x[3]);
+    if (vx[2]) x[0] = P::fold(x[0], x[2]);
+    A a = x[0];
+    int va = vx[0];
 #pragma unroll
     for (int h = 1; h < 32; h <<= 1) {
         A pa = __shfl_down_sync(0xffffffffu, a, h);
@@ -129,8 +138,8 @@ template <class T> __device__ __forceinline__ T plain_add(T x, T y) {
 // Per-warp shared memory of k_red_rowst: the window ring, the segment's
 // window-sum slots, one window's leaf-sum slots, the ring's descriptions.
 template <class T> constexpr size_t rst_warp_smem() {
-    return ((size_t)RST_STAGES * rst_win_phys<T>() * sizeof(T) + 64 * sizeof(T) * 2 +
-            (size_t)RST_STAGES * sizeof(RstMeta) + 64 * 2 + 127) / 128 * 128;  // each warp's ring 128-byte aligned
+    return ((size_t)RST_STAGES * rst_win_phys<T>() * sizeof(T) + (64 + 128) * sizeof(T) +
+            (size_t)RST_STAGES * sizeof(RstMeta) + 64 + 128 + 127) / 128 * 128;  // each warp's ring 128-byte aligned
 }
 template <class T> constexpr size_t rst_smem() { return (size_t)rst_warps<T>() * rst_warp_smem<T>(); }
 
@@ -144,22 +153,27 @@ __global__ void __launch_bounds__(32 * rst_warps<typename DT<CD>::T>()) k_red_ro
     constexpr int PADE = rst_pad<T>();
     constexpr int WP = rst_win_phys<T>();
     constexpr int NWARP = rst_warps<T>();
+    constexpr int WIN = rst_win<T>();
+    constexpr int CPL = WIN / 64 / 32;   // candidate positions per lane
+    constexpr int LPL = WIN / 128 / 32;  // leaves per lane in a full power-of-two window
+    constexpr int DREG = LPL == 2 ? 6 : 5;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    unsigned char* mine = smem_raw + (size_t)warp * rst_warp_smem<T>();
-    T* ring = reinterpret_cast<T*>(mine);
+    unsigned char* wbase = smem_raw + (size_t)warp * rst_warp_smem<T>();
+    T* ring = reinterpret_cast<T*>(wbase);
     A* uslot = reinterpret_cast<A*>(ring + (size_t)RST_STAGES * WP);   // [64]
-    A* lslot = uslot + 64;                                               // [64]
-    RstMeta* meta = reinterpret_cast<RstMeta*>(lslot + 64);              // [RST_STAGES]
+    A* lslot = uslot + 64;                                               // [128]
+    RstMeta* meta = reinterpret_cast<RstMeta*>(lslot + 128);             // [RST_STAGES]
     uint8_t* uvalid = reinterpret_cast<uint8_t*>(meta + RST_STAGES);     // [64]
-    uint8_t* lvalid = uvalid + 64;                                       // [64]
+    uint8_t* lvalid = uvalid + 64;                                       // [128]
     const int Dw = d.Dw, Dl = d.Dl, NW = 1 << Dw;
     const int64_t nseg = (int64_t)1 << d.K;
     const int64_t nunits = d.nout * nseg;
     const int64_t gw = (int64_t)blockIdx.x * NWARP + warp, GW = (int64_t)gridDim.x * NWARP;
     const int64_t myunits = nunits > gw ? (nunits - gw + GW - 1) / GW : 0;
     const int64_t Q = myunits * NW;
-    for (int i = lane; i < 64; i += 32) { uvalid[i] = 0; lvalid[i] = 0; }
+    for (int i = lane; i < 64; i += 32) uvalid[i] = 0;
+    for (int i = lane; i < 128; i += 32) lvalid[i] = 0;
     const T* a = reinterpret_cast<const T*>(d.a);
 
     // the unit last issued: its base, and its windows' nodes (lane l holds
@@ -191,12 +205,12 @@ __global__ void __launch_bounds__(32 * rst_warps<typename DT<CD>::T>()) k_red_ro
             if (live) {
                 T* sb = ring + (size_t)(q % RST_STAGES) * WP;
                 const T* src = a + cbase + noff;
-                if (nlen == RST_WIN) {
+                if (nlen == WIN) {
                     // a full window: chunk lane + 32 i holds elements
                     // 128 i / VE ... of block (lane * VE) / 128 + ..., so both
                     // addresses advance by a constant per i
 #pragma unroll
-                    for (int i = 0; i < RST_WIN / (32 * VE); ++i) {
+                    for (int i = 0; i < WIN / (32 * VE); ++i) {
                         const int e = (lane + 32 * i) * VE;
                         cp_async16(sb + e + PADE * (e >> 7), src + e);
                     }
@@ -216,12 +230,14 @@ __global__ void __launch_bounds__(32 * rst_warps<typename DT<CD>::T>()) k_red_ro
         }
         cp_async_commit();  // one group per window, empty or not
     };
-    // the leaves that start at this lane's two candidate positions (2*lane
-    // and 2*lane + 1, 64 elements apart) for the current window length: one
-    // 128-element leaf per lane in a regular window
+    // the leaves that start at this lane's CPL candidate positions (CPL*lane
+    // + h, 64 elements apart) for the current window length: LPL
+    // 128-element leaves per lane in a full power-of-two window
     int cachedL = -1;
-    int loff[2] = {0, 0}, llen[2] = {0, 0}, lsi[2] = {0, 0};
-    bool lhas[2];
+    int loff[CPL], llen[CPL], lsi[CPL];
+    bool lhas[CPL];
+#pragma unroll
+    for (int h = 0; h < CPL; ++h) { loff[h] = 0; llen[h] = 0; lsi[h] = 0; lhas[h] = false; }
     for (int s = 0; s < RST_STAGES - 1; ++s) issue(s);
     for (int64_t q = 0; q < Q; ++q) {
         issue(q + RST_STAGES - 1);
@@ -235,8 +251,8 @@ __global__ void __launch_bounds__(32 * rst_warps<typename DT<CD>::T>()) k_red_ro
                 cachedL = L;
                 const int ncand = (L + 63) / 64;
 #pragma unroll
-                for (int h = 0; h < 2; ++h) {
-                    const int c = 2 * lane + h;
+                for (int h = 0; h < CPL; ++h) {
+                    const int c = CPL * lane + h;
                     lhas[h] = false;
                     if (c < ncand) {
                         const int mm = c * 64;
@@ -254,17 +270,20 @@ __global__ void __launch_bounds__(32 * rst_warps<typename DT<CD>::T>()) k_red_ro
                     }
                 }
             }
-            // a full power-of-two window: lane l sums leaf l, whose slot is l
-            const bool regular = L == RST_WIN && Dl == 5;
-            A mine = A{};
-            bool mine_set = false;
+            // a full power-of-two window: lane l sums leaves LPL*l + i, whose
+            // slots are their indices
+            const bool regular = L == WIN && Dl == DREG;
+            A mine[LPL];
+            bool mine_set[LPL];
+#pragma unroll
+            for (int i = 0; i < LPL; ++i) { mine[i] = A{}; mine_set[i] = false; }
             // each lane sums its leaves with plain adds, 8 independent
             // accumulator chains; leaves whose sum is NaN are queued and
             // then summed again with the engine's NaN rule, 8 lanes per
             // leaf, so one NaN does not hold the whole warp in a serial
             // replay
 #pragma unroll
-            for (int h = 0; h < 2; ++h) {
+            for (int h = 0; h < CPL; ++h) {
                 const int off = loff[h], len = llen[h];
                 const bool fast = lhas[h] && len == PW_BLOCK && (off & (PW_BLOCK - 1)) == 0;
                 bool redo = lhas[h] && !fast;
@@ -286,8 +305,8 @@ __global__ void __launch_bounds__(32 * rst_warps<typename DT<CD>::T>()) k_red_ro
                                             plain_add(plain_add(r[4], r[5]), plain_add(r[6], r[7])));
                     if (res == res) {
                         if (regular) {
-                            mine = res;
-                            mine_set = true;
+                            mine[h / 2] = res;  // candidate CPL*lane + h starts leaf (CPL*lane + h) / 2
+                            mine_set[h / 2] = true;
                         } else {
                             lslot[lsi[h]] = res;
                             lvalid[lsi[h]] = 1;
@@ -337,21 +356,25 @@ __global__ void __launch_bounds__(32 * rst_warps<typename DT<CD>::T>()) k_red_ro
             __syncwarp();
             A wsum;
             if (regular) {
-                // the 32 leaf sums of a perfect tree, folded across lanes
-                // left operand first
-                if (!mine_set) mine = lslot[lane];
+                // the leaf sums of a perfect tree: the lane's own leaves
+                // first, then across lanes, left operand first
+#pragma unroll
+                for (int i = 0; i < LPL; ++i)
+                    if (!mine_set[i]) mine[i] = lslot[LPL * lane + i];
+                A v = mine[0];
+                if constexpr (LPL == 2) v = P::fold(mine[0], mine[1]);
 #pragma unroll
                 for (int hh = 1; hh < 32; hh <<= 1) {
-                    const A o = __shfl_down_sync(0xffffffffu, mine, hh);
-                    if ((lane & (2 * hh - 1)) == 0) mine = P::fold(mine, o);
+                    const A o = __shfl_down_sync(0xffffffffu, v, hh);
+                    if ((lane & (2 * hh - 1)) == 0) v = P::fold(v, o);
                 }
-                wsum = mine;
+                wsum = v;
             } else {
                 wsum = warp_slot_tree<P>(lslot, lvalid, Dl, lane);
             }
             __syncwarp();
-            lvalid[lane] = 0;
-            lvalid[lane + 32] = 0;
+#pragma unroll
+            for (int i = 0; i < 4; ++i) lvalid[lane + 32 * i] = 0;
             if (lane == 0) {
                 uslot[p] = wsum;
                 uvalid[p] = 1;
@@ -768,7 +791,7 @@ static cudaError_t launch_row_wide(const RedDesc& din, cudaStream_t s) {
     if constexpr (rowst_type_ok(OP, CD)) {
         if (!row_wide_ok(din, (int)sizeof(T))) return cudaErrorNotSupported;
         RedDesc d = din;
-        if (!rst_plan(d.w, d.K, RST_WIN, &d.Dw, &d.Dl)) return cudaErrorNotSupported;
+        if (!rst_plan(d.w, d.K, rst_win<T>(), &d.Dw, &d.Dl)) return cudaErrorNotSupported;
         const int64_t units = d.nout << d.K;
         auto k = k_red_rowst<OP, CD>;
         const size_t smem = rst_smem<T>();

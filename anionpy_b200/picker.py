@@ -141,9 +141,30 @@ class Mlp:
         return losses
 
 
+def stream_schedules() -> np.ndarray:
+    """Schedules a call may take inside a mixed stream: at least 256 threads'
+    worth of block tile, at most 1024 16-byte units of work per tile, no
+    reduction split. The autotuner times a call alone (many copies of it),
+    where long tiles amortise per-tile costs; in a persistent kernel shared
+    by thousands of different calls, long tiles and split reductions made the
+    whole stream slower (10,000-call stream, every call on one schedule: these
+    7 schedules took 11.2-11.9 ms, tiles of 2048-16384 units 12.7-15.9 ms,
+    block tile 128 14.5-21.3 ms, each split variant 1.4-3.2 ms more), so the
+    picker chooses among these."""
+    from ._batch import BLOCK_TILES, ELEMS_PER_THREAD, RED_SPLITS, VEC_WIDTHS, schedule_index
+    keep = []
+    for bt in BLOCK_TILES:
+        for vw in VEC_WIDTHS:
+            for ept in ELEMS_PER_THREAD:
+                if bt >= 256 and bt * vw * ept <= 1024:
+                    keep.append(schedule_index(bt, vw, ept, RED_SPLITS[0]))
+    return np.array(sorted(keep))
+
+
 class SchedulePicker:
-    """Picks one schedule per call: the network's argmin, or the autotuner for
-    calls outside the training feature box."""
+    """Picks one schedule per call: the network's argmin (over `allowed`
+    schedules when given), or the autotuner for calls outside the training
+    feature box."""
 
     def __init__(self, path=DEFAULT_WEIGHTS):
         d = np.load(path)
@@ -155,15 +176,16 @@ class SchedulePicker:
     def predict(self, feats: np.ndarray) -> np.ndarray:
         return self.mlp.forward(feats)
 
-    def pick(self, batch: Batch, fallback=True, reps=3) -> np.ndarray:
+    def pick(self, batch: Batch, fallback=True, reps=3, allowed=None) -> np.ndarray:
         f = features(batch)
         pred = self.predict(f)
-        picks = np.argmin(pred, axis=1)
+        cols = np.arange(pred.shape[1]) if allowed is None else np.asarray(allowed)
+        picks = cols[np.argmin(pred[:, cols], axis=1)]
         outside = np.any((f < self.lo - 1e-6) | (f > self.hi + 1e-6), axis=1)
         self.fallbacks = int(outside.sum())
         if fallback:
             for i in np.nonzero(outside)[0]:
-                picks[i] = int(np.argmin(batch.time_call(int(i), reps=reps)))
+                picks[i] = int(cols[np.argmin(batch.time_call(int(i), scheds=cols, reps=reps))])
         return picks
 
 

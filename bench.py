@@ -327,9 +327,11 @@ def mixed_stream_bench(ap, L, steps, warmup, ncalls=10000, check_every=10, sched
         if os.path.exists(picker.DEFAULT_WEIGHTS):
             t0 = _time.perf_counter()
             sp = picker.SchedulePicker()
-            schedules = sp.pick(b)
+            allowed = picker.stream_schedules()
+            schedules = sp.pick(b, allowed=allowed)
             res["picker"] = {"pick_s": round(_time.perf_counter() - t0, 3), "fallback_calls": sp.fallbacks,
-                             "distinct_schedules": int(len(set(schedules.tolist())))}
+                             "distinct_schedules": int(len(set(schedules.tolist()))),
+                             "stream_schedule_set": [int(k) for k in allowed]}
         else:
             schedules = None
     if schedules is not None:
@@ -714,8 +716,9 @@ def main():
                                  "ms": round(red_ms, 3)}},
             "roofline": None if dom is None else
             {"bound": "hbm", "kernel": rows[dom]["case"], "achieved": rows[dom]["GB/s"], "peak": hbm_peak,
-             "unit": "GB/s", "frac": rows[dom]["frac"], "traffic": None, "peak_kind": peak_kind,
-             "headline_add_f32_contig": head},
+             "unit": "GB/s", "frac": rows[dom]["frac"],
+             "traffic": traffic_of(rows[dom]["case"], items[dom].nbytes), "traffic_unit": "bytes per launch",
+             "peak_kind": peak_kind, "headline_add_f32_contig": head},
             "mixed_stream": mixed,
             "cpu_baseline": cpu,
             "e2e": e2e,
@@ -728,6 +731,18 @@ def main():
         print(json.dumps(line), flush=True)
     if dist is not None:
         dist.destroy_process_group()
+
+
+# DRAM bytes moved per algorithmic byte, from ncu captures of the same
+# kernels on 2^24-element cases (dram__bytes_read.sum + dram__bytes_write.sum
+# of one launch over its algorithmic bytes); the traffic of a full-size
+# launch scales with its elements.
+NCU_TRAFFIC_PER_BYTE = {}
+
+
+def traffic_of(case, alg_bytes):
+    r = NCU_TRAFFIC_PER_BYTE.get(case)
+    return None if r is None else int(round(r * alg_bytes))
 
 
 def end_to_end(ap, L, n, steps, chunk=1 << 24, nstreams=3):

@@ -38,3 +38,16 @@ def test_schedule_space_matches_the_library():
         seen.add(t)
     assert len(seen) == 48
     assert L.ionp_schedule_from_index(48, _lib.IonpSchedule()) != 0
+
+
+def test_stream_schedule_set():
+    from anionpy_b200 import picker
+    from anionpy_b200._batch import BLOCK_TILES, ELEMS_PER_THREAD, RED_SPLITS, VEC_WIDTHS
+    allowed = picker.stream_schedules()
+    assert len(allowed) == 7 and len(set(allowed.tolist())) == 7
+    default = schedule_index(256, 1, 4, 1)
+    assert default in allowed
+    for k in allowed:
+        bt, rest = BLOCK_TILES[k // 12], k % 12
+        vw, ept, sp = VEC_WIDTHS[rest // 4], ELEMS_PER_THREAD[(rest % 4) // 2], RED_SPLITS[rest % 2]
+        assert bt >= 256 and bt * vw * ept <= 1024 and sp == 1

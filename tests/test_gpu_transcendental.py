@@ -145,3 +145,20 @@ def test_log_fpe():
     with ap.errstate(invalid="raise"):
         with pytest.raises(FloatingPointError, match="invalid value encountered in log"):
             ap.log(ap.from_numpy(np.array([0.0, -1.0], np.float32)))
+
+
+@pytest.mark.parametrize("fn", ["exp", "log", "sin"])
+@pytest.mark.parametrize("dt", [np.float32, np.float64], ids=lambda d: np.dtype(d).name)
+def test_strided_slices(fn, dt):
+    """Step-2 and step-3 slices (the one-strided-run path) give the same
+    bits as the contiguous kernel, and log's FPE categories still fire."""
+    x = inputs(fn, dt, 30000 if dt == np.float64 else 1 << 18, 9)
+    d = ap.from_numpy(x)
+    full = getattr(ap, fn)(d).get()
+    for step in (2, 3):
+        got = getattr(ap, fn)(d[::step]).get()
+        assert_bits_equal(got, full[::step], f"{fn} {np.dtype(dt).name} step {step}")
+    if fn == "log":
+        with ap.errstate(divide="raise"):
+            with pytest.raises(FloatingPointError, match="divide by zero encountered in log"):
+                ap.log(ap.from_numpy(np.array([1.0, 5.0, 0.0, 7.0], dt))[::2])
