@@ -253,9 +253,49 @@ def study(ntrain, ntest, seed=7, reps=3, epochs=60, out=DEFAULT_WEIGHTS, log=pri
     return res, (Xtr, Ttr, Xte, Tte)
 
 
+def stream_sweep(ncalls=10000, seed=7, steps=4, warmup=2):
+    """Device milliseconds of the mixed stream (persistent kernel, CUDA graph)
+    with every call on one schedule, for each of the 48, and with the learned
+    picks over all schedules and over `stream_schedules()`."""
+    import anionpy_b200 as ap
+    from . import workloads
+    check = _lib.check
+    L = _lib.lib()
+    calls, _ = workloads.mixed_stream(ncalls=ncalls, seed=seed)
+    pools = workloads.DevicePools(ap, pool_elems=1 << 22, seed=17)
+    b, _ = workloads.build_batch(ap, calls, pools)
+    e0, e1 = ctypes.c_void_p(), ctypes.c_void_p()
+    check(L.ionp_event_create(ctypes.byref(e0)))
+    check(L.ionp_event_create(ctypes.byref(e1)))
+
+    def timed(sched):
+        b.set_schedules(sched)
+        for _ in range(warmup):
+            b.run(graph=True)
+        check(L.ionp_device_synchronize())
+        check(L.ionp_event_record(e0, None))
+        for _ in range(steps):
+            b.run(graph=True)
+        check(L.ionp_event_record(e1, None))
+        check(L.ionp_device_synchronize())
+        ms = ctypes.c_float()
+        check(L.ionp_event_elapsed_ms(e0, e1, ctypes.byref(ms)))
+        return {"ms": round(ms.value / steps, 3), "tiles": b.info()["tiles"]}
+
+    n = len(b)
+    res = {f"schedule_{k}": timed(np.full(n, k)) for k in range(NUM_SCHEDULES)}
+    if os.path.exists(DEFAULT_WEIGHTS):
+        sp = SchedulePicker()
+        res["learned_all"] = timed(sp.pick(b, fallback=False))
+        res["learned_stream_set"] = timed(sp.pick(b, fallback=False, allowed=stream_schedules()))
+    return res
+
+
 def main():
     ap_ = argparse.ArgumentParser()
     sub = ap_.add_subparsers(dest="cmd", required=True)
+    t = sub.add_parser("stream", help="time the mixed stream under every schedule")
+    t.add_argument("--calls", type=int, default=10000)
     s = sub.add_parser("study")
     s.add_argument("--train", type=int, default=50000)
     s.add_argument("--test", type=int, default=5000)
@@ -265,6 +305,9 @@ def main():
     s.add_argument("--report", default=None, help="write the regret summary (JSON) here")
     s.add_argument("--dump", default=None, help="save the timing dataset (npz) here")
     args = ap_.parse_args()
+    if args.cmd == "stream":
+        print(json.dumps(stream_sweep(args.calls), indent=1))
+        return
     res, data = study(args.train, args.test, reps=args.reps, epochs=args.epochs, out=args.out)
     print(json.dumps(res, indent=1))
     if args.report:

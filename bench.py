@@ -736,8 +736,13 @@ def main():
 # DRAM bytes moved per algorithmic byte, from ncu captures of the same
 # kernels on 2^24-element cases (dram__bytes_read.sum + dram__bytes_write.sum
 # of one launch over its algorithmic bytes); the traffic of a full-size
-# launch scales with its elements.
-NCU_TRAFFIC_PER_BYTE = {}
+# launch scales with its elements. sin/float64/step2: 268.5 MB read (every
+# other 8-byte element of each sector is skipped, so reads are twice the
+# logical bytes) + 78.1 MB written of 268.4 MB algorithmic; writes still
+# held in the 126 MB L2 when the 2^24-element launch ends are not counted,
+# so at full size the ratio approaches 1.5. add/float32/contig: 134.2 MB
+# read + 29.2 MB written of 201.3 MB (the same L2 effect on writes).
+NCU_TRAFFIC_PER_BYTE = {"sin/float64/step2": 1.2913, "add/float32/contig": 0.8117}
 
 
 def traffic_of(case, alg_bytes):
