@@ -5,20 +5,21 @@
 // warp touches whole 128-byte lines.
 //
 //  k_red_rowst : float add, numpy's pairwise tree (ufunc.rs:6416-6448).
-//                Each run segment is cut at a fixed depth Dw of its split
-//                tree into windows of at most 16 KiB; a window is a subtree,
-//                so its leaves never cross a window edge. cp.async streams
-//                windows into a 4-stage shared-memory ring (every 128-element
-//                leaf block padded by 8 elements, so that the 8 lanes that
-//                sum one leaf's 8 interleaved accumulators and the 4 leaves
-//                a warp sums at once fall in distinct banks). Eight lanes sum
-//                one leaf: lane k folds accumulator k (elements k, k+8, ...)
-//                in order, the group combines ((r0+r1)+(r2+r3))+((r4+r5)+
-//                (r6+r7)) with shuffles and lane 0 adds the len % 8 tail.
-//                Leaf sums go to a perfect-binary-tree slot array that warp 0
-//                folds level by level with shuffles (left operand first);
-//                window sums go to the segment's slot array, folded the same
-//                way after its last window.
+//                One warp per run segment. The segment is cut at a fixed
+//                depth Dw of its split tree into windows of at most 4096
+//                elements; a window is a subtree, so its leaves never cross a
+//                window edge. The warp streams its windows through its own
+//                2-stage cp.async ring (16 bytes of padding after every 128
+//                elements, so lanes reading different leaves hit distinct
+//                banks). One lane sums one 128-element leaf: its 8
+//                interleaved accumulators (elements k, k+8, ...) run as 8
+//                independent chains of plain IEEE adds, combined
+//                ((r0+r1)+(r2+r3))+((r4+r5)+(r6+r7)); a leaf whose sum comes
+//                out NaN is queued by warp ballot and summed again with the
+//                engine's NaN-payload rule, 8 lanes per leaf. Leaf sums of a
+//                full power-of-two window fold across lanes with shuffles,
+//                others through a perfect-binary-tree slot array (left
+//                operand first); window sums fold the same way per segment.
 //  k_red_rowco : the order-free folds: integer add/multiply (wrapping),
 //                bitwise and/or/xor, integer max/min, and float max/min,
 //                whose only order dependence is that the first NaN in fold
