@@ -148,8 +148,8 @@ def stream_schedules() -> np.ndarray:
     where long tiles amortise per-tile costs; in a persistent kernel shared
     by thousands of different calls, long tiles and split reductions made the
     whole stream slower (10,000-call stream, every call on one schedule: these
-    7 schedules took 11.2-11.9 ms, tiles of 2048-16384 units 12.7-15.9 ms,
-    block tile 128 14.5-21.3 ms, each split variant 1.4-3.2 ms more), so the
+    7 schedules took 11.2-12.3 ms, tiles of 2048-16384 units 12.6-15.9 ms,
+    block tile 128 14.6-21.2 ms, each split variant 1.5-2.6 ms more), so the
     picker chooses among these."""
     from ._batch import BLOCK_TILES, ELEMS_PER_THREAD, RED_SPLITS, VEC_WIDTHS, schedule_index
     keep = []
