@@ -1,8 +1,8 @@
-// Unary op table (ufunc.rs:3824-3975 unary_op, 4237-4367 math_unary_f32/f64)
-// and the transcendental kernels it calls.
+// Unary op table (ufunc.rs:3824-3975 unary_op, 4237-4367 math_unary_f32/f64);
+// exp/log/sin are the C-library restatements of ionp_libm.cuh.
 #pragma once
 #include "ionp_scalar.cuh"
-#include "ionp_transcendental.cuh"
+#include "ionp_libm.cuh"
 
 namespace ionp {
 
@@ -28,15 +28,15 @@ template <int OP, int CD> struct UnOp {
     }
     static __device__ __forceinline__ float f32op(float x) {
         if constexpr (OP == OP_SQRT) return x_sqrt(x);
-        else if constexpr (OP == OP_EXP) return cr_expf(x);
-        else if constexpr (OP == OP_LOG) return cr_logf(x);
-        else return cr_sinf(x);
+        else if constexpr (OP == OP_EXP) return lm::exp32(x);
+        else if constexpr (OP == OP_LOG) return lm::log32(x);
+        else return lm::sin32(x);
     }
     static __device__ __forceinline__ double f64op(double x) {
         if constexpr (OP == OP_SQRT) return x_sqrt(x);
-        else if constexpr (OP == OP_EXP) return cr_exp(x);
-        else if constexpr (OP == OP_LOG) return cr_log(x);
-        else return cr_sin(x);
+        else if constexpr (OP == OP_EXP) return lm::exp64(x);
+        else if constexpr (OP == OP_LOG) return lm::log64(x);
+        else return lm::sin64(x);
     }
     // detect_sqrt / detect_log (fpe.rs:359-396): x < 0 -> invalid,
     // log(0) -> divide.
