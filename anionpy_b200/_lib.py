@@ -66,6 +66,8 @@ _SIGS = {
                            ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int64)],
     "ionp_binary": [ctypes.c_int32, _P, _P, _P, _P, ctypes.POINTER(ctypes.c_uint32), ctypes.c_void_p],
     "ionp_unary": [ctypes.c_int32, _P, _P, _P, ctypes.POINTER(ctypes.c_uint32), ctypes.c_void_p],
+    "ionp_binary_nowait": [ctypes.c_int32, _P, _P, _P, _P, ctypes.c_void_p, ctypes.c_void_p],
+    "ionp_unary_nowait": [ctypes.c_int32, _P, _P, _P, ctypes.c_void_p, ctypes.c_void_p],
     "ionp_cast": [_P, _P, ctypes.c_void_p],
     "ionp_reduce": [ctypes.c_int32, _P, ctypes.POINTER(ctypes.c_int32), ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
                     ctypes.c_void_p, _P, _P, ctypes.c_void_p],

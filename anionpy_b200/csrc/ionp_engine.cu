@@ -465,6 +465,9 @@ int32_t FlagWord::read(uint32_t* host) {
     *host = *t_pinned_flag;
     return IONP_OK;
 }
+int32_t FlagWord::read_async(uint32_t* host) {
+    return cuda_err(cudaMemcpyAsync(host, d, sizeof(uint32_t), cudaMemcpyDeviceToHost, s), "fpe flag copy");
+}
 FlagWord::~FlagWord() {
     if (d) scratch_free(d, s);
 }
@@ -706,8 +709,8 @@ int32_t ionp_alloc_trim(void) {
     return IONP_OK;
 }
 
-int32_t ionp_binary(int32_t op, const IonpArr* a, const IonpArr* b, IonpArr* out, const IonpArr* where, uint32_t* fpe,
-                    IonpStream stream) {
+static int32_t binary_call(int32_t op, const IonpArr* a, const IonpArr* b, IonpArr* out, const IonpArr* where,
+                           uint32_t* fpe, bool nowait, IonpStream stream) {
     int32_t st;
     if ((st = check_arr(a, "a")) || (st = check_arr(b, "b")) || (st = check_arr(out, "out"))) return st;
     if (where && (st = check_arr(where, "where"))) return st;
@@ -800,12 +803,22 @@ int32_t ionp_binary(int32_t op, const IonpArr* a, const IonpArr* b, IonpArr* out
     }
     if (want) {
         if (numel(a) == 0 || numel(b) == 0) return IONP_OK;
-        return fw.read(fpe);
+        return fw.deliver(fpe, nowait);
     }
     return IONP_OK;
 }
 
-int32_t ionp_unary(int32_t op, const IonpArr* a, IonpArr* out, const IonpArr* where, uint32_t* fpe, IonpStream stream) {
+int32_t ionp_binary(int32_t op, const IonpArr* a, const IonpArr* b, IonpArr* out, const IonpArr* where, uint32_t* fpe,
+                    IonpStream stream) {
+    return binary_call(op, a, b, out, where, fpe, false, stream);
+}
+int32_t ionp_binary_nowait(int32_t op, const IonpArr* a, const IonpArr* b, IonpArr* out, const IonpArr* where,
+                           uint32_t* fpe, IonpStream stream) {
+    return binary_call(op, a, b, out, where, fpe, true, stream);
+}
+
+static int32_t unary_call(int32_t op, const IonpArr* a, IonpArr* out, const IonpArr* where, uint32_t* fpe, bool nowait,
+                          IonpStream stream) {
     int32_t st;
     if ((st = check_arr(a, "a")) || (st = check_arr(out, "out"))) return st;
     if (where && (st = check_arr(where, "where"))) return st;
@@ -823,8 +836,16 @@ int32_t ionp_unary(int32_t op, const IonpArr* a, IonpArr* out, const IonpArr* wh
     if (want && (st = fw.open(s))) return st;
     if (fpe) *fpe = 0;
     if ((st = launch_ew(false, op, cd, rd, a, nullptr, out, where, fw.d, want, s))) return st;
-    if (want) return fw.read(fpe);
+    if (want) return fw.deliver(fpe, nowait);
     return IONP_OK;
+}
+
+int32_t ionp_unary(int32_t op, const IonpArr* a, IonpArr* out, const IonpArr* where, uint32_t* fpe, IonpStream stream) {
+    return unary_call(op, a, out, where, fpe, false, stream);
+}
+int32_t ionp_unary_nowait(int32_t op, const IonpArr* a, IonpArr* out, const IonpArr* where, uint32_t* fpe,
+                          IonpStream stream) {
+    return unary_call(op, a, out, where, fpe, true, stream);
 }
 
 int32_t ionp_cast(const IonpArr* a, IonpArr* out, IonpStream stream) {

@@ -92,6 +92,10 @@ int32_t run_row(RedDesc& d, cudaStream_t s) {
     int K = 0;
     if (w > SEG_MAX) {
         while (*seg_lengths(w, K).rbegin() > SEG_MAX) ++K;
+        // the top pass folds at most 2^(2 TOP_CHUNK_LOG) partials per output
+        // (runs of up to 2^38 elements; only zero-stride views get longer)
+        if (K > 2 * TOP_CHUNK_LOG)
+            return set_err(IONP_ERR_VALUE, "reduction run of " + std::to_string(w) + " elements is longer than the 2^38 this engine folds");
     }
     // more parallel units when there are few outputs and long runs: the
     // wide-row kernels take a warp (float add) or a CTA per unit
@@ -100,7 +104,7 @@ int32_t run_row(RedDesc& d, cudaStream_t s) {
         if (rowst_type_ok(d.op, d.cd)) want = 148 * 16;
         else if (rowco_type_ok(d.op, d.cd)) want = 148 * RCO_CTAS;
     }
-    while ((d.nout << K) < want && *seg_lengths(w, K + 1).begin() >= 4096 && K < 20) ++K;
+    while ((d.nout << K) < want && *seg_lengths(w, K + 1).begin() >= 4096 && K < 20 && K < 2 * TOP_CHUNK_LOG) ++K;
     auto lens = seg_lengths(w, K);
     int64_t maxlen = *lens.rbegin();
     std::map<int64_t, int> memo;

@@ -69,6 +69,10 @@ struct FlagWord {
     cudaStream_t s = nullptr;
     int32_t open(cudaStream_t st);
     int32_t read(uint32_t* host);
+    // stream-ordered copy into a caller's (pinned) host word; no wait
+    int32_t read_async(uint32_t* host);
+    // read() or read_async() by the call's mode
+    int32_t deliver(uint32_t* host, bool nowait) { return nowait ? read_async(host) : read(host); }
     ~FlagWord();
 };
 

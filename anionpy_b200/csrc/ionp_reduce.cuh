@@ -398,25 +398,46 @@ __global__ void __launch_bounds__(RED_THREADS, 4) k_red_row(RedDesc d) {
 
 // Top of a split tree: per output, combine its 2^K partials as a perfect
 // binary tree (adjacent pairs, left operand first), then seed and store.
+// The partials are folded in chunks of 2^KC (each chunk is a perfect
+// subtree of the same tree); the 2^(K - KC) chunk results then fold as the
+// tree's top levels, so shared memory stays at TOP_CHUNK + 2^(K - KC) values
+// for any K <= 2 TOP_CHUNK_LOG.
+constexpr int TOP_CHUNK_LOG = 11;
+__host__ __device__ constexpr int top_chunk_log(int K) { return K < TOP_CHUNK_LOG ? K : TOP_CHUNK_LOG; }
+template <class A>
+__host__ __device__ constexpr size_t row_top_smem(int K) {
+    return (((size_t)1 << top_chunk_log(K)) + ((size_t)1 << (K - top_chunk_log(K)))) * sizeof(A);
+}
 template <int OP, int CD>
 __global__ void __launch_bounds__(RED_THREADS) k_red_row_top(RedDesc d) {
     typedef RPol<OP, CD> P;
     typedef typename P::A A;
     extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int kc = top_chunk_log(d.K);
+    const int csize = 1 << kc, nchunk = 1 << (d.K - kc);
     A* v = reinterpret_cast<A*>(smem_raw);
-    const int nseg = 1 << d.K;
+    A* top = v + csize;
+    const int64_t nseg = (int64_t)1 << d.K;
     for (int64_t o = blockIdx.x; o < d.nout; o += gridDim.x) {
-        const A* part = reinterpret_cast<const A*>(d.scratch) + o * nseg;
-        for (int s = threadIdx.x; s < nseg; s += blockDim.x) v[s] = part[s];
-        __syncthreads();
-        for (int half = 1; half < nseg; half <<= 1) {
-            for (int s = threadIdx.x * 2 * half; s < nseg; s += blockDim.x * 2 * half) v[s] = P::fold(v[s], v[s + half]);
+        for (int c = 0; c < nchunk; ++c) {
+            const A* part = reinterpret_cast<const A*>(d.scratch) + o * nseg + (int64_t)c * csize;
+            for (int s = threadIdx.x; s < csize; s += blockDim.x) v[s] = part[s];
+            __syncthreads();
+            for (int half = 1; half < csize; half <<= 1) {
+                for (int s = threadIdx.x * 2 * half; s < csize; s += blockDim.x * 2 * half) v[s] = P::fold(v[s], v[s + half]);
+                __syncthreads();
+            }
+            if (threadIdx.x == 0) top[c] = v[0];
+            __syncthreads();
+        }
+        for (int half = 1; half < nchunk; half <<= 1) {
+            for (int s = threadIdx.x * 2 * half; s < nchunk; s += blockDim.x * 2 * half) top[s] = P::fold(top[s], top[s + half]);
             __syncthreads();
         }
         if (threadIdx.x == 0) {
             int64_t in_off, out_off;
             kept_offsets(d, o, &in_off, &out_off);
-            store_cast<CD>(d.o, out_off, d.odt, P::finish(v[0], d.has_seed, d.seed));
+            store_cast<CD>(d.o, out_off, d.odt, P::finish(top[0], d.has_seed, d.seed));
         }
         __syncthreads();
     }

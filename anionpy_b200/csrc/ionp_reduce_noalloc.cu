@@ -226,7 +226,7 @@ extern "C" int32_t ionp_reduce_noalloc(int32_t op, const IonpArr* a, const int32
     const size_t acc = (cd == DT_F16 && op == OP_ADD) ? 4 : (size_t)dt_bytes(cd);
     int K = 0;
     if (w > SEG_LIMIT)
-        while (*lengths_at(w, K).rbegin() > SEG_LIMIT) ++K;
+        while (*lengths_at(w, K).rbegin() > SEG_LIMIT && K <= 2 * TOP_CHUNK_LOG) ++K;
     auto fits = [&](int k) { return k == 0 || (size_t)(d.nout << k) * acc <= (size_t)IONP_NOALLOC_SCRATCH_BYTES; };
     if (!fits(K))
         return set_err(IONP_ERR_VALUE, "ionp_reduce_noalloc: the partial results of this reduction (" +

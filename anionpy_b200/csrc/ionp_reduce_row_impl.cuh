@@ -19,7 +19,10 @@ static cudaError_t row_t2(const RedDesc& d, int tpr, size_t smem, int grid, cuda
         case 32: k_red_row<OP, CD, 32, C><<<grid, RED_THREADS, smem, s>>>(d); break;
         default: {
             auto k = k_red_row<OP, CD, 256, C>;
-            if (smem > 48 * 1024) cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+            if (smem > 48 * 1024) {
+                cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+                if (e != cudaSuccess) return e;
+            }
             k<<<grid, RED_THREADS, smem, s>>>(d);
         } break;
     }
@@ -39,11 +42,10 @@ static cudaError_t row_top_t(const RedDesc& d, cudaStream_t s) {
             return cudaGetLastError();
         }
     }
-    size_t smem = ((size_t)1 << d.K) * sizeof(A);
+    if (d.K > 2 * TOP_CHUNK_LOG) return cudaErrorInvalidValue;   // planners cap K far below this
+    const size_t smem = row_top_smem<A>(d.K);                    // at most 32 KiB
     int grid = (int)(d.nout < 148 * 8 ? d.nout : 148 * 8);
-    auto k = k_red_row_top<OP, CD>;
-    if (smem > 48 * 1024) cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    k<<<grid, RED_THREADS, smem, s>>>(d);
+    k_red_row_top<OP, CD><<<grid, RED_THREADS, smem, s>>>(d);
     count_launch();
     return cudaGetLastError();
 }

@@ -202,16 +202,17 @@ class ReduceCase:
         self._o = self.out._desc()
         self.L = L
 
-    def launch(self):
+    def launch(self, stream=None):
         from anionpy_b200 import _lib
         if self.op == "argmax":
-            _lib.check(self.L.ionp_argext(1, ctypes.byref(self._a), self.ax, int(self.keepdims), ctypes.byref(self._o), None))
+            _lib.check(self.L.ionp_argext(1, ctypes.byref(self._a), self.ax, int(self.keepdims), ctypes.byref(self._o),
+                                          stream))
         else:
             from anionpy_b200 import BINARY_OPS
             _lib.check(self.L.ionp_reduce(BINARY_OPS[self.op], ctypes.byref(self._a), self.axes, self.naxes,
                                           int(self.keepdims), -1,
                                           self.init.ctypes.data if self.init is not None else None,
-                                          None, ctypes.byref(self._o), None))
+                                          None, ctypes.byref(self._o), stream))
 
     def check(self):
         """Whole result against the oracle, bit for bit."""
@@ -417,135 +418,195 @@ class Clocks:
 
 
 # ---------------------------------------------------------------------------
-# CPU side: the oracle (the restatement of the reference's engine)
+# CPU side: the oracle (the restatement of the reference's engine) on one
+# pinned core, over a bounded sample of the GPU step's own case list, with
+# NumPy timed beside it
 # ---------------------------------------------------------------------------
-def cpu_sample_cases(n):
+CPU_ELEMS = 1 << 20      # elements per operand of each element-wise case (side 1024)
+CPU_RED_SCALE = 64       # leading extent of each reduction input divided by this
+
+
+def red_out_bytes(host, op, axis, keepdims):
+    n_out = 1 if axis is None else host.size // host.shape[axis]
+    if op == "argmax":
+        return 8 * n_out
+    return n_out * (8 if host.dtype.kind in "iu" else host.dtype.itemsize)
+
+
+def cpu_cases(n=CPU_ELEMS, red_scale=CPU_RED_SCALE):
+    """The GPU step's 111 cases on host data of the same distributions:
+    every element-wise op x dtype x layout with n elements per operand (the
+    transposed case a (sqrt n, sqrt n) view, the step-2 case a slice of a 2n
+    base) and the 27 reductions on inputs whose leading extent is divided by
+    red_scale. Items: (name, kind, op, operands, kwargs, logical bytes)."""
     rng = np.random.default_rng(99)
+    side = int(round(n ** 0.5))
     out = []
     for dt in DTYPES:
+        isz = np.dtype(dt).itemsize
         isint = dt.startswith("int")
-        a = gen_block("int" if isint else "float", dt, n, rng)
-        b = gen_block("divisor" if isint else "float", dt, n, rng)
+        a = gen_block("int" if isint else "float", dt, 2 * n, rng)
+        b = gen_block("divisor" if isint else "float", dt, 2 * n, rng)
+        views = {"contig": (a[:n], b[:n]), "transposed": (a[:n].reshape(side, side).T, b[n:].reshape(side, side)),
+                 "step2": (a[::2], b[::2])}
         for op in (BIN_OPS_INT if isint else BIN_OPS_FLT):
-            out.append((op, [a, b], 3 * n * np.dtype(dt).itemsize))
+            for lay in LAYOUTS:
+                out.append((f"{op}/{dt}/{lay}", "binary", op, views[lay], {}, 3 * n * isz))
         if not isint:
             for fn in UN_OPS:
-                out.append((fn, [gen_block(fn, dt, n, rng)], 2 * n * np.dtype(dt).itemsize))
-    return out
-
-
-def cpu_reduce_cases(scale):
-    """The reduction inputs with the leading extent divided by `scale`."""
-    out = []
-    for tag, host, keepdims, initial in reduce_inputs(scale):
+                u = gen_block(fn, dt, 2 * n, rng)
+                uv = {"contig": u[:n], "transposed": u[:n].reshape(side, side).T, "step2": u[::2]}
+                for lay in LAYOUTS:
+                    out.append((f"{fn}/{dt}/{lay}", "unary", fn, (uv[lay],), {}, 2 * n * isz))
+    for tag, host, keepdims, initial in reduce_inputs(red_scale):
         for op in RED_OPS:
             for axis in RED_AXES:
-                nb = host.nbytes
-                out.append((op, host, axis, keepdims, initial if op != "argmax" else None, nb))
+                ax = None if axis is None else axis % host.ndim
+                nb = host.nbytes + red_out_bytes(host, op, ax, keepdims)
+                if op == "argmax":
+                    out.append((f"argmax/{tag}/axis={axis}", "argmax", op, (host,),
+                                {"axis": axis, "keepdims": keepdims}, nb))
+                else:
+                    kw = {"axis": axis, "keepdims": keepdims}
+                    if initial is not None:
+                        kw["initial"] = initial
+                    out.append((f"{op}.reduce/{tag}/axis={axis}", "reduce", op, (host,), kw, nb))
     return out
 
 
-def _split_axis(a, axis):
-    """The axis along which independent outputs can be split between threads."""
-    if axis is None or a.ndim == 1:
-        return None
-    ax = axis % a.ndim
-    return 0 if ax != 0 else 1
+def run_oracle(case):
+    from oracle import oracle as O
+    _, kind, op, ops, kw, _ = case
+    if kind == "binary":
+        return O.binary(op, *ops)
+    if kind == "unary":
+        return O.unary(op, ops[0])
+    if kind == "argmax":
+        return O.argext("argmax", ops[0], **kw)
+    return O.reduce(op, ops[0], **kw)
 
 
-def time_oracle_reduce(cases, threads):
-    """Oracle reductions; the outputs are split between threads along a kept
-    axis (each output's fold order is unchanged); all-axis reductions run on
-    one thread (one ordered fold)."""
+def run_numpy(case):
+    _, kind, op, ops, kw, _ = case
+    with np.errstate(all="ignore"):
+        if kind == "binary":
+            return getattr(np, op)(*ops)
+        if kind == "unary":
+            return getattr(np, op)(ops[0])
+        if kind == "argmax":
+            return np.argmax(ops[0], **kw)
+        return getattr(np, op).reduce(ops[0], **kw)
+
+
+def time_pass(cases, runner):
+    """(logical bytes, seconds) of one pass over the cases."""
+    t0 = time.perf_counter()
+    nb = 0
+    for c in cases:
+        runner(c)
+        nb += c[5]
+    return nb, time.perf_counter() - t0
+
+
+def time_all_cores_elementwise(cases, threads):
+    """GB/s of the element-wise cases with each case's output rows split
+    between `threads` threads (element-wise results do not depend on the
+    split; reductions are left out: their fold order must not change)."""
     from concurrent.futures import ThreadPoolExecutor
     from oracle import oracle as O
-    O.lib()
-    total = 0
+    ew = [c for c in cases if c[1] in ("binary", "unary")]
+    nb = 0
     t0 = time.perf_counter()
     with ThreadPoolExecutor(max_workers=threads) as ex:
-        for op, a, axis, keepdims, initial, nb in cases:
-            sa = _split_axis(a, axis)
-            def one(x):
-                if op == "argmax":
-                    return O.argext("argmax", x, axis=axis, keepdims=keepdims)
-                kw = {"keepdims": keepdims}
-                if initial is not None:
-                    kw["initial"] = initial
-                return O.reduce(op, x, axis=axis, **kw)
-            if sa is None:
-                ex.submit(one, a).result()
-            else:
-                n = a.shape[sa]
-                parts = [(i * n // threads, (i + 1) * n // threads) for i in range(threads)]
-                fs = []
-                for lo, hi in parts:
-                    if hi > lo:
-                        idx = [slice(None)] * a.ndim
-                        idx[sa] = slice(lo, hi)
-                        fs.append(ex.submit(one, a[tuple(idx)]))
-                for f in fs:
-                    f.result()
-            total += nb
-    dt = time.perf_counter() - t0
-    return total, dt
-
-
-def time_oracle(cases, threads):
-    from concurrent.futures import ThreadPoolExecutor
-    from oracle import oracle as O
-    O.lib()
-    total_bytes = 0
-    t0 = time.perf_counter()
-    with ThreadPoolExecutor(max_workers=threads) as ex:
-        for op, ops, nbytes in cases:
-            n = ops[0].size
-            chunks = [(i * n // threads, (i + 1) * n // threads) for i in range(threads)]
-            if len(ops) == 2:
-                fs = [ex.submit(O.binary, op, ops[0][lo:hi], ops[1][lo:hi]) for lo, hi in chunks]
-            else:
-                fs = [ex.submit(O.unary, op, ops[0][lo:hi]) for lo, hi in chunks]
-            for f in fs:
+        for name, kind, op, ops, kw, b in ew:
+            m = ops[0].shape[0]
+            parts = [(i * m // threads, (i + 1) * m // threads) for i in range(threads)]
+            fn = (lambda lo, hi: O.binary(op, ops[0][lo:hi], ops[1][lo:hi])) if kind == "binary" else \
+                (lambda lo, hi: O.unary(op, ops[0][lo:hi]))
+            for f in [ex.submit(fn, lo, hi) for lo, hi in parts if hi > lo]:
                 f.result()
-            total_bytes += nbytes
-    dt = time.perf_counter() - t0
-    return total_bytes / dt / 1e9, dt
+            nb += b
+    return nb / (time.perf_counter() - t0) / 1e9
 
 
-def cpu_step(cases, rcases, threads):
-    """GB/s of one pass over the sampled element-wise and reduction cases."""
-    v, dt = time_oracle(cases, threads)
-    rb, rdt = time_oracle_reduce(rcases, threads)
-    eb = v * dt * 1e9
-    return (eb + rb) / (dt + rdt) / 1e9, dt + rdt
+def host_info():
+    model = None
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                model = line.split(":", 1)[1].strip()
+                break
+    except OSError:
+        pass
+    try:
+        glibc = os.confstr("CS_GNU_LIBC_VERSION")
+    except (ValueError, OSError):
+        glibc = None
+    return {"cpu_model": model, "nproc": os.cpu_count(), "glibc": glibc, "numpy": np.__version__}
+
+
+def cpu_measure(steps, warmup, numpy_steps=1, all_cores=True):
+    """The oracle and NumPy over cpu_cases(), this thread pinned to one core
+    (the reference's CPU path is single-threaded); the median step of each.
+    Returns (cpu_baseline dict, oracle seconds per step)."""
+    from oracle import oracle as O
+    O.lib()
+    cases = cpu_cases()
+    before = os.sched_getaffinity(0)
+    core = min(before)
+    os.sched_setaffinity(0, {core})
+    try:
+        for _ in range(warmup):
+            time_pass(cases, run_oracle)
+        runs = [time_pass(cases, run_oracle) for _ in range(max(steps, 1))]
+        nps = [time_pass(cases, run_numpy) for _ in range(max(numpy_steps, 1))]
+    finally:
+        os.sched_setaffinity(0, before)
+    nb = runs[0][0]
+    secs = statistics.median(r[1] for r in runs)
+    np_secs = statistics.median(r[1] for r in nps)
+    res = {"value": round(nb / secs / 1e9, 3), "unit": "GB/s", "cores": 1, "kind": "port",
+           "sample": f"the GPU step's {len(cases)} cases (84 element-wise: every op x dtype x layout at "
+                     f"{CPU_ELEMS} elements per operand, the transposed case a (1024, 1024) view, the step-2 case a "
+                     f"slice of a {2 * CPU_ELEMS}-element base; the 27 reductions on inputs with the leading extent "
+                     f"/ {CPU_RED_SCALE}), {nb / 1e9:.2f} GB of logical bytes per step, one thread pinned to core "
+                     f"{core}, median of {len(runs)} steps of {secs:.2f} s",
+           "restatement": "oracle/ionp_oracle.cpp, the C++ restatement of ionp-core's loops (the Rust crate "
+                          "cannot be built here: no cargo)",
+           "numpy": {"value": round(nb / np_secs / 1e9, 3), "unit": "GB/s", "cores": 1,
+                     "what": f"NumPy {np.__version__} ufuncs on the same sample, same pinned core"},
+           "host": host_info()}
+    if all_cores:
+        th = len(before)
+        res["all_cores_elementwise"] = {"value": round(time_all_cores_elementwise(cases, th), 3), "unit": "GB/s",
+                                        "cores": th, "what": "the 84 element-wise cases only, rows split between threads"}
+    return res, secs
+
+
+def workload_config(n, world, reduce_scale):
+    return {"workload": "large element-wise sweep (2^28 elements per operand: 6 binary ufuncs x int32/int64, "
+                        "5 x float32/float64, exp/log/sin x float32/float64; contiguous, transposed "
+                        "(16384,16384) view, step-2 slice) + reductions (add.reduce, maximum.reduce, argmax "
+                        "over axis 0/-1/None of float32 (8192,32768), float64 (4096,4096,16) keepdims "
+                        "initial=0.0, int64 (2^27,))",
+            "elements_per_operand": n, "cases": 111, "reduce_scale": reduce_scale,
+            "l2": "inputs 1-8 GiB per operand > 126 MB L2, no flush", "parallelism": f"replicas x{world}"}
 
 
 def reference_arm(args):
     rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
     if rank != 0:
         return
-    threads = os.cpu_count() or 1
-    n = 1 << 21
-    red_scale = 64
-    cases = cpu_sample_cases(n)
-    rcases = cpu_reduce_cases(red_scale)
-    for _ in range(args.warmup):
-        time_oracle(cases[:2], threads)
-    vals = []
-    for _ in range(args.steps):
-        v, _ = cpu_step(cases, rcases, threads)
-        vals.append(v)
-    value = statistics.median(vals)
-    sample = (f"{len(cases)} contiguous sweep cases x {n} elements (2^21 of 2^28) and the {len(rcases)} reductions "
-              f"on inputs with the leading extent / {red_scale}, per step, split over {threads} threads")
+    cpu, secs = cpu_measure(args.steps, args.warmup, numpy_steps=1)
     line = {
-        "metric": METRIC, "value": round(value, 3), "unit": "GB/s", "n_gpus": args.gpus, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
+        "metric": METRIC, "value": cpu["value"], "unit": "GB/s", "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(secs * 1e3, 1), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "mixed(int32,int64,f32,f64)", "data": "synthetic",
-        "config": {"workload": "large element-wise sweep (contiguous cases) + reductions (bounded CPU sample)",
-                   "elements": n, "reduce_scale": red_scale},
+        "config": workload_config(args.elements, world, 1),
         "impl": "reference",
-        "cpu_baseline": {"value": round(value, 3), "unit": "GB/s", "cores": threads, "kind": "port", "sample": sample},
-        "e2e": {"value": round(value, 3), "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "cpu_baseline": cpu,
+        "e2e": {"value": cpu["value"], "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
 
@@ -693,25 +754,14 @@ def main():
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
-        sample_n = 1 << 22
-        v, secs = cpu_step(cpu_sample_cases(sample_n), cpu_reduce_cases(32), 1)
-        cpu = {"value": round(v, 3), "unit": "GB/s", "cores": 1, "kind": "port",
-               "sample": f"the {len(cpu_sample_cases(16))} contiguous sweep cases at {sample_n} elements each (2^22 of 2^28) "
-                         f"and the 27 reductions on inputs with the leading extent / 32, single thread, "
-                         f"{secs:.1f} s of CPU work"}
+        cpu, _ = cpu_measure(2, 1, numpy_steps=1)
 
     if rank == 0:
         line = {
             "metric": METRIC, "value": round(value, 2), "unit": "GB/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(total_ms / args.steps, 3), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "mixed(int32,int64,f32,f64)", "data": "synthetic",
-            "config": {"workload": "large element-wise sweep (2^28 elements per operand: 6 binary ufuncs x int32/int64, "
-                                   "5 x float32/float64, exp/log/sin x float32/float64; contiguous, transposed "
-                                   "(16384,16384) view, step-2 slice) + reductions (add.reduce, maximum.reduce, argmax "
-                                   "over axis 0/-1/None of float32 (8192,32768), float64 (4096,4096,16) keepdims "
-                                   "initial=0.0, int64 (2^27,))",
-                       "elements_per_operand": n, "cases": len(items), "reduce_scale": args.reduce_scale,
-                       "l2": "inputs 1-8 GiB per operand > 126 MB L2, no flush", "parallelism": f"replicas x{world}"},
+            "config": workload_config(n, world, args.reduce_scale),
             "parts": {"elementwise": {"GB/s": round(sweep_b / (sweep_ms / 1e3) / 1e9, 1) if sweep_ms else None,
                                       "frac": round(sweep_b / (sweep_ms / 1e3) / 1e9 / hbm_peak, 3) if sweep_ms else None,
                                       "ms": round(sweep_ms, 3)},
@@ -757,91 +807,198 @@ def traffic_of(case, alg_bytes):
     return None if r is None else int(round(r * alg_bytes))
 
 
-def end_to_end(ap, L, n, steps, chunk=1 << 24, nstreams=3):
-    """GB/s of the contiguous cases through the C ABI (ionp_binary /
-    ionp_unary), inputs copied from pinned host buffers and every result read
-    back inside the timed region. Each case is cut into chunks issued round
-    robin on `nstreams` streams (copy in, compute, copy out per chunk), so the
-    host-to-device copies, the kernels and the device-to-host copies of
-    neighbouring chunks overlap."""
+def end_to_end(ap, L, n, steps, nstreams=3, chunk=1 << 24):
+    """GB/s of the step's 111 cases through the C ABI from pinned host
+    buffers: every case copies its operands host->device, runs, and copies
+    its result back, all inside the timed region; the logical bytes counted
+    are the step's (the same as `value`). Element-wise calls go through
+    ionp_binary_nowait / ionp_unary_nowait with a pinned FPE word each, so
+    the reference's detectors run on every call without a host wait.
+
+    Cases are issued round robin on `nstreams` streams so that one case's
+    copy in, another's kernels and a third's copy out overlap; contiguous
+    cases are further cut into `chunk`-element pieces. A transposed case
+    copies both (16384, 16384) operand bases whole, a step-2 case both 2^29
+    bases (the host-side views a caller would pass), so these move more PCIe
+    bytes than they have logical bytes. The reductions copy each input once
+    per step and read back all nine results."""
     from anionpy_b200 import _lib
-    itemmax = 8
-    hp = [ctypes.c_void_p() for _ in range(3)]
-    for h in hp:
-        _lib.check(L.ionp_host_alloc(ctypes.byref(h), n * itemmax))
+    side = int(round(n ** 0.5))
+    P = ctypes.c_void_p
+
+    def pinned(nbytes):
+        h = P()
+        _lib.check(L.ionp_host_alloc(ctypes.byref(h), nbytes))
+        return h
+
+    hA, hB = pinned(2 * n * 8), pinned(2 * n * 8)
     rng = np.random.default_rng(5)
+    for h in (hA, hB):
+        blk = gen_block("float", np.float64, 1 << 22, rng).view(np.uint8)
+        arr = np.ctypeslib.as_array((ctypes.c_uint8 * (2 * n * 8)).from_address(h.value))
+        for off in range(0, arr.size, blk.size):
+            arr[off: off + blk.size] = blk[: arr.size - off]
+    hO = [pinned(n * 8) for _ in range(nstreams)]
+    nfpe = 8192
+    hF = pinned(4 * nfpe)
+    fpe_words = np.ctypeslib.as_array((ctypes.c_uint32 * nfpe).from_address(hF.value))
+    streams = [P() for _ in range(nstreams)]
+    for st in streams:
+        _lib.check(L.ionp_stream_create(ctypes.byref(st)))
+    dA = [ap.empty((2 * n * 8,), np.uint8) for _ in range(nstreams)]
+    dB = [ap.empty((2 * n * 8,), np.uint8) for _ in range(nstreams)]
+    dO = [ap.empty((n * 8,), np.uint8) for _ in range(nstreams)]
+
+    def view(buf, dt, shape, strides):
+        return ap.ndarray(buf._buf, shape, dt, strides, 0)
+
+    kout = (ctypes.c_int64 * 2)()
+
+    def order_k(ops, shape):
+        descs = [o._desc() for o in ops]
+        arr = (ctypes.POINTER(_lib.IonpArr) * len(descs))(*[ctypes.pointer(d) for d in descs])
+        sh = (ctypes.c_int64 * len(shape))(*shape)
+        _lib.check(L.ionp_order_k_strides(len(descs), arr, len(shape), sh, kout))
+        return tuple(kout[i] for i in range(len(shape)))
+
+    fpe_i = [0]
+
+    def next_fpe():
+        p = hF.value + 4 * (fpe_i[0] % nfpe)
+        fpe_i[0] += 1
+        return p
+
+    def launch(kind, op, ops, out, sh):
+        code = ap.BINARY_OPS[op] if kind == 2 else ap.UNARY_OPS[op]
+        descs = [o._desc() for o in ops]
+        do = out._desc()
+        if kind == 2:
+            _lib.check(L.ionp_binary_nowait(code, ctypes.byref(descs[0]), ctypes.byref(descs[1]), ctypes.byref(do),
+                                            None, next_fpe(), sh))
+        else:
+            _lib.check(L.ionp_unary_nowait(code, ctypes.byref(descs[0]), ctypes.byref(do), None, next_fpe(), sh))
+
     todo = []
     for dt in DTYPES:
         isint = dt.startswith("int")
         for op in (BIN_OPS_INT if isint else BIN_OPS_FLT):
-            todo.append((op, dt, 2))
+            for lay in LAYOUTS:
+                todo.append((op, dt, 2, lay))
         if not isint:
             for fn in UN_OPS:
-                todo.append((fn, dt, 1))
-    chunk = min(chunk, n)
-    streams = [ctypes.c_void_p() for _ in range(nstreams)]
-    for st in streams:
-        _lib.check(L.ionp_stream_create(ctypes.byref(st)))
-    # per stream: chunk buffers for a, b, out (sized for 8-byte elements)
-    bufs = [[ap.empty((chunk * itemmax,), np.uint8) for _ in range(3)] for _ in range(nstreams)]
-    # host data (one block tiled)
-    for i, h in enumerate(hp[:2]):
-        blk = gen_block("float", np.float64, 1 << 22, rng).view(np.uint8)
-        arr = np.ctypeslib.as_array((ctypes.c_uint8 * (n * itemmax)).from_address(h.value))
-        for off in range(0, arr.size, blk.size):
-            arr[off: off + blk.size] = blk[: arr.size - off]
+                for lay in LAYOUTS:
+                    todo.append((fn, dt, 1, lay))
+    rot = [0]
 
-    def desc(buf, dt, m):
-        v = ap.ndarray(buf._buf, (m,), dt, (1,), 0)
-        return v._desc()
-
-    def one_case(op, dt, k):
+    def one_case(op, dt, k, lay):
+        """(h2d, d2h, logical) bytes of one element-wise case"""
         isz = np.dtype(dt).itemsize
-        code = ap.BINARY_OPS[op] if k == 2 else ap.UNARY_OPS[op]
-        nb = 0
-        for ci, lo in enumerate(range(0, n, chunk)):
-            m = min(chunk, n - lo)
-            sidx = ci % nstreams
-            sh = streams[sidx]
-            ba, bb, bo = bufs[sidx]
-            L.ionp_memcpy(ba.data_ptr, hp[0].value + lo * isz, m * isz, 0, sh)
-            da, do = desc(ba, dt, m), desc(bo, dt, m)
+        h2d = d2h = 0
+        if lay == "contig":
+            for lo in range(0, n, chunk):
+                m = min(chunk, n - lo)
+                i = rot[0] % nstreams
+                rot[0] += 1
+                sh = streams[i]
+                ops = []
+                for hsrc, dbuf in ((hA, dA[i]), (hB, dB[i]))[:k]:
+                    L.ionp_memcpy(dbuf.data_ptr, hsrc.value + lo * isz, m * isz, 0, sh)
+                    ops.append(view(dbuf, dt, (m,), (1,)))
+                    h2d += m * isz
+                out = view(dO[i], dt, (m,), (1,))
+                launch(k, op, ops, out, sh)
+                L.ionp_memcpy(hO[i].value + lo * isz, dO[i].data_ptr, m * isz, 1, sh)
+                d2h += m * isz
+            return h2d, d2h, (k + 1) * n * isz
+        i = rot[0] % nstreams
+        rot[0] += 1
+        sh = streams[i]
+        base = n if lay == "transposed" else 2 * n
+        for hsrc, dbuf in ((hA, dA[i]), (hB, dB[i]))[:k]:
+            L.ionp_memcpy(dbuf.data_ptr, hsrc.value, base * isz, 0, sh)
+            h2d += base * isz
+        if lay == "transposed":
+            ops = [view(dA[i], dt, (side, side), (1, side))]
             if k == 2:
-                L.ionp_memcpy(bb.data_ptr, hp[1].value + lo * isz, m * isz, 0, sh)
-                db = desc(bb, dt, m)
-                _lib.check(L.ionp_binary(code, ctypes.byref(da), ctypes.byref(db), ctypes.byref(do), None, None, sh))
-            else:
-                _lib.check(L.ionp_unary(code, ctypes.byref(da), ctypes.byref(do), None, None, sh))
-            L.ionp_memcpy(hp[2].value + lo * isz, bo.data_ptr, m * isz, 1, sh)
-            nb += (k + 1) * m * isz
-        return nb
+                ops.append(view(dB[i], dt, (side, side), (side, 1)))
+            shape = (side, side)
+        else:
+            ops = [view(buf, dt, (n,), (2,)) for buf in (dA[i], dB[i])[:k]]
+            shape = (n,)
+        out = view(dO[i], dt, shape, order_k(ops, shape))
+        launch(k, op, ops, out, sh)
+        L.ionp_memcpy(hO[i].value, dO[i].data_ptr, n * isz, 1, sh)
+        d2h += n * isz
+        return h2d, d2h, (k + 1) * n * isz
 
-    e0, e1 = ctypes.c_void_p(), ctypes.c_void_p()
+    # reductions: pinned copies of the three inputs, one device input each,
+    # preallocated outputs for the nine reductions of each input
+    red = []
+    for tag, host, keepdims, initial in reduce_inputs(1):
+        hin = pinned(host.nbytes)
+        np.ctypeslib.as_array((ctypes.c_uint8 * host.nbytes).from_address(hin.value))[:] = host.reshape(-1).view(np.uint8)
+        dev = ap.empty(host.shape, host.dtype)
+        cases = [ReduceCase(ap, L, f"{op}/{tag}/{axis}", op, dev, host, axis, keepdims,
+                            initial if op != "argmax" else None) for op in RED_OPS for axis in RED_AXES]
+        outs = [pinned(max(c.out_bytes, 8)) for c in cases]
+        red.append((host, hin, dev, cases, outs))
+
+    def reductions():
+        h2d = d2h = lg = 0
+        for host, hin, dev, cases, outs in red:
+            i = rot[0] % nstreams
+            rot[0] += 1
+            sh = streams[i]
+            L.ionp_memcpy(dev.data_ptr, hin.value, host.nbytes, 0, sh)
+            h2d += host.nbytes
+            for c, ho in zip(cases, outs):
+                c.launch(sh)
+                L.ionp_memcpy(ho.value, c.out.data_ptr, c.out_bytes, 1, sh)
+                d2h += c.out_bytes
+                lg += c.nbytes
+        return h2d, d2h, lg
+
+    e0 = P()
     L.ionp_event_create(ctypes.byref(e0))
-    L.ionp_event_create(ctypes.byref(e1))
-    for op, dt, k in todo[:2]:  # untimed: first launches, stream set-up
-        one_case(op, dt, k)
+    for t in todo[:2]:      # untimed: first launches, stream set-up
+        one_case(*t)
+    reductions()
     L.ionp_device_synchronize()
-    h2d = d2h = 0
-    nbytes = 0
-    L.ionp_event_record(e0, None)
+    h2d = d2h = logical = 0
+    L.ionp_event_record(e0, streams[0])
     for _ in range(steps):
-        for op, dt, k in todo:
-            isz = np.dtype(dt).itemsize
-            nbytes += one_case(op, dt, k)
-            h2d += k * n * isz
-            d2h += n * isz
+        for t in todo:
+            a, b, c = one_case(*t)
+            h2d += a
+            d2h += b
+            logical += c
+        a, b, c = reductions()
+        h2d += a
+        d2h += b
+        logical += c
+    # the streams are non-blocking: the region ends at the last of the
+    # per-stream end events
+    ends = [P() for _ in streams]
+    for ev, st in zip(ends, streams):
+        L.ionp_event_create(ctypes.byref(ev))
+        L.ionp_event_record(ev, st)
     L.ionp_device_synchronize()
-    L.ionp_event_record(e1, None)
-    ms = ctypes.c_float()
-    L.ionp_event_elapsed_ms(e0, e1, ctypes.byref(ms))
-    for h in hp:
+    ms = ctypes.c_float(0.0)
+    for ev in ends:
+        m = ctypes.c_float()
+        _lib.check(L.ionp_event_elapsed_ms(e0, ev, ctypes.byref(m)))
+        ms.value = max(ms.value, m.value)
+        L.ionp_event_destroy(ev)
+    flagged = int(np.count_nonzero(fpe_words))
+    for h in [hA, hB, hF] + hO + [r[1] for r in red] + [o for r in red for o in r[4]]:
         L.ionp_host_free(h)
     for st in streams:
         L.ionp_stream_destroy(st)
-    return {"value": round(nbytes / (ms.value / 1e3) / 1e9, 3), "unit": "GB/s",
+    return {"value": round(logical / (ms.value / 1e3) / 1e9, 3), "unit": "GB/s",
             "h2d_bytes_per_step": h2d // steps, "d2h_bytes_per_step": d2h // steps,
-            "pipeline": f"{nstreams} streams, {chunk}-element chunks"}
+            "cases": len(todo) + sum(len(r[3]) for r in red), "steps": steps,
+            "pipeline": f"{nstreams} streams, contiguous cases in {chunk}-element chunks",
+            "fpe_words_set": flagged}
 
 
 if __name__ == "__main__":

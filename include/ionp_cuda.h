@@ -123,6 +123,18 @@ int32_t ionp_binary(int32_t op, const IonpArr* a, const IonpArr* b, IonpArr* out
  * (ufunc.rs:4606). Same out/where/fpe conventions as ionp_binary. */
 int32_t ionp_unary(int32_t op, const IonpArr* a, IonpArr* out, const IonpArr* where, uint32_t* fpe,
                    IonpStream stream);
+/* ionp_binary / ionp_unary that never wait for the stream. `fpe` (NULL, or
+ * a host word, best from ionp_host_alloc) receives the same detector bits,
+ * written by a copy in stream order: read it after the stream has
+ * synchronized. For ops without a detector it is set to 0 before the call
+ * returns. No counterpart in the reference, whose calls are synchronous;
+ * these let a caller overlap copies and kernels of consecutive calls and
+ * still get the reference's FPE categories (fpe_check_after_call,
+ * ionp-py/src/lib.rs:9077-9138). */
+int32_t ionp_binary_nowait(int32_t op, const IonpArr* a, const IonpArr* b, IonpArr* out, const IonpArr* where,
+                           uint32_t* fpe, IonpStream stream);
+int32_t ionp_unary_nowait(int32_t op, const IonpArr* a, IonpArr* out, const IonpArr* where, uint32_t* fpe,
+                          IonpStream stream);
 /* Element-wise dtype conversion/copy of `a` into `out` (same shape, any
  * strides): Buffer::cast_to (ionp-core/src/buffer.rs:210). */
 int32_t ionp_cast(const IonpArr* a, IonpArr* out, IonpStream stream);
@@ -158,6 +170,12 @@ int32_t ionp_reduce(int32_t op, const IonpArr* a, const int32_t* axes, int32_t n
  *     65536 elements).
  *   - The first call on a device looks up the array's device address with
  *     that device current; make that first call before any stream capture.
+ *     With CUDA's lazy module loading (the default) that first call also
+ *     loads the library's kernels and the array onto the device, which the
+ *     driver allocates: a caller that reserves its whole memory budget up
+ *     front should make one warm-up call (any supported reduction) first.
+ *   - The address is cached per device for the life of the process; do not
+ *     reset the device (cudaDeviceReset) while using this entry point.
  *   - All calls share the one array: calls that overlap on the GPU (on
  *     different streams, or from several threads) race on it. Serialise them
  *     on one stream. */

@@ -19,6 +19,7 @@ import numpy as np
 import pytest
 
 from anionpy_b200 import _lib
+from oracle import oracle as O
 from tests._util import assert_bits_equal
 
 ap = pytest.importorskip("anionpy_b200")
@@ -52,6 +53,18 @@ def _stats():
     s = (ctypes.c_uint64 * 4)()
     _lib.check(_lib.lib().ionp_alloc_stats(s))
     return list(s)
+
+
+def noalloc(op, a, axis, keepdims, initial, out_dtype):
+    """ionp_reduce_noalloc into a fresh output of out_dtype; (status, out)."""
+    L = _bind()
+    cax, nax = _axes(axis, a.ndim)
+    out = _out_for(a, list(cax)[:nax], keepdims, out_dtype)
+    init_buf = None if initial is None else np.array([initial], dtype=out_dtype)
+    da, do = a._desc(), out._desc()
+    st = L.ionp_reduce_noalloc(OPS[op], ctypes.byref(da), cax, nax, int(keepdims),
+                               None if init_buf is None else init_buf.ctypes.data, ctypes.byref(do), None)
+    return st, out
 
 
 def run_both(op, a, axis, keepdims=False, initial=None):
@@ -117,6 +130,50 @@ def test_noalloc_matches_reduce_twice(case):
     for call in range(2):
         want, got = run_both(op, a, axis, keepdims, initial)
         assert_bits_equal(got, want, f"{op} {np.dtype(dt).name}{shape} axis={axis} call {call + 1}")
+
+
+@pytest.mark.parametrize("case", CASES, ids=lambda c: f"{c[0]}-{np.dtype(c[1]).name}-{c[2]}-{c[3]}")
+def test_noalloc_matches_oracle(case):
+    """The same cases against the oracle (the CPU restatement of the
+    reference's reduce_axis), bit for bit."""
+    op, dt, shape, axis, keepdims, initial = case
+    host = _data(dt, shape, 5)
+    kw = {"axis": axis, "keepdims": keepdims}
+    if initial is not None:
+        kw["initial"] = initial
+    want = np.asarray(O.reduce(op, host, **kw))
+    st, out = noalloc(op, ap.from_numpy(host), axis, keepdims, initial, want.dtype)
+    _lib.check(st)
+    assert_bits_equal(out.get().reshape(want.shape), want, f"{op} {np.dtype(dt).name}{shape} vs oracle")
+
+
+def test_noalloc_widening_and_zero_d():
+    """int8 and bool add.reduce widen to int64 on load; a 0-d input reduces
+    to itself plus the seed. Each against ionp_reduce and the oracle."""
+    rng = np.random.default_rng(8)
+    for host in (rng.integers(-128, 128, (3, 200001)).astype(np.int8), rng.integers(0, 2, (2, 150001)).astype(np.bool_)):
+        a = ap.from_numpy(host)
+        want, got = run_both("add", a, 1)
+        assert_bits_equal(got, want, f"add {host.dtype} vs ionp_reduce")
+        assert_bits_equal(got, np.asarray(O.reduce("add", host, axis=1)), f"add {host.dtype} vs oracle")
+    for v in (np.array(2.5), np.array(-7, np.int32)):
+        want = np.asarray(O.reduce("add", v, axis=None))
+        st, out = noalloc("add", ap.from_numpy(v), None, False, None, want.dtype)
+        _lib.check(st)
+        assert_bits_equal(out.get().reshape(want.shape), want, f"0-d {v.dtype}")
+
+
+def test_noalloc_long_zero_stride_run():
+    """A zero-stride view with a 2^32-element run (no memory behind it) splits
+    into 2^16 segments: the top pass folds 2^16 partials per output, far more
+    than shared memory holds at once. Pairwise sums of a constant power-of-two
+    multiple are exact, so the result is known in closed form."""
+    for dt, v in ((np.float64, 1.5), (np.float32, 1.0)):
+        base = ap.from_numpy(np.array([v], dt))
+        view = ap.ndarray(base._buf, (1 << 32,), dt, strides=(0,), offset=0)
+        want, got = run_both("add", view, 0)
+        assert_bits_equal(got, want, f"{np.dtype(dt).name} 2^32 zero-stride run vs ionp_reduce")
+        assert float(got) == v * 2.0 ** 32, (float(got), v * 2.0 ** 32)
 
 
 def test_noalloc_sequence_of_different_calls():
