@@ -160,6 +160,57 @@ k_bin_nd(EwDesc d, uint32_t* flags) {
     if constexpr (FPE) flush_flags(bits, flags);
 }
 
+// One merged dim with any element strides, operands and result in the loop
+// dtypes, no mask (a step-k slice, a reversed view): U elements of each
+// operand loaded per thread before any arithmetic, so 2U loads are in
+// flight, and no per-element index unravelling.
+// streaming (evict-first) scalar load / store where the type has one
+template <class T> __device__ __forceinline__ T ld_cs(const T* p) {
+    if constexpr (sizeof(T) >= 4) return __ldcs(p);
+    else return *p;
+}
+template <class T> __device__ __forceinline__ void st_cs(T* p, T v) {
+    if constexpr (sizeof(T) >= 4) __stcs(p, v);
+    else *p = v;
+}
+
+template <int OP, int CD, bool FPE>
+__global__ void __launch_bounds__(EW_THREADS)
+k_bin_run(EwDesc d, uint32_t* flags) {
+    typedef typename DT<CD>::T T;
+    typedef BinOp<OP, CD> Op;
+    typedef typename Op::R R;
+    constexpr int U = sizeof(T) >= 8 ? 4 : 8;
+    const T* pa = reinterpret_cast<const T*>(d.a.p);
+    const T* pb = reinterpret_cast<const T*>(d.b.p);
+    R* po = reinterpret_cast<R*>(d.o);
+    const int64_t sa = d.a.st[0], sb = d.b.st[0], so = d.so[0], n = d.n;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    uint32_t bits = 0;
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    for (; i + (U - 1) * stride < n; i += U * stride) {
+        T x[U], y[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            x[u] = ld_cs(pa + (i + u * stride) * sa);
+            y[u] = ld_cs(pb + (i + u * stride) * sb);
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const R r = Op::apply(x[u], y[u]);
+            if constexpr (FPE) bits |= fpe_bits<OP, CD>(x[u], y[u], r);
+            st_cs(po + (i + u * stride) * so, r);
+        }
+    }
+    for (; i < n; i += stride) {
+        const T x = pa[i * sa], y = pb[i * sb];
+        const R r = Op::apply(x, y);
+        if constexpr (FPE) bits |= fpe_bits<OP, CD>(x, y, r);
+        po[i * so] = r;
+    }
+    if constexpr (FPE) flush_flags(bits, flags);
+}
+
 // Two merged dims whose operands disagree on which dim is contiguous (a
 // transposed view against a C-ordered one): 32 x 32 tiles staged through
 // shared memory. Each operand is read along its own contiguous dim, the
@@ -214,6 +265,85 @@ k_bin_tr(EwDesc d, uint32_t* flags) {
                 if constexpr (FPE) bits |= fpe_bits<OP, CD>(x, y, v);
                 po[(i0 + r) * d.so[0] + (j0 + c) * d.so[1]] = v;
             }
+        }
+        __syncthreads();
+    }
+    if constexpr (FPE) flush_flags(bits, flags);
+}
+
+// The same two-dim case for whole tiles whose rows are 16-byte aligned:
+// TILE x TILE tiles (64 for 4-byte types, 32 for 8-byte ones), every global
+// load and store a 16-byte vector along that array's own contiguous dim
+// (VW elements), so a warp moves 512 bytes per instruction; each thread has
+// all its vectors of both operands in flight before the tile's barrier.
+// Shared rows are padded by one element: the column-wise scatter of a
+// column-contiguous operand hits each bank at most twice, the row-wise reads
+// of the compute phase not at all.
+template <class T> struct TrV {
+    static constexpr int VW = 16 / (int)sizeof(T);
+    static constexpr int TILE = sizeof(T) == 4 ? 64 : 32;
+    static constexpr int TPR = TILE / VW;                 // threads per tile row
+    static constexpr int PASS = TILE / (EW_THREADS / TPR);
+};
+template <class T> __device__ __forceinline__ void trv_load(T (*sm)[TrV<T>::TILE + 1], const T* p, int64_t s0,
+                                                          int64_t s1, int64_t i0, int64_t j0) {
+    typedef TrV<T> V;
+    const int tid = threadIdx.x;
+    const int lane_v = (tid % V::TPR) * V::VW, line = tid / V::TPR;
+    if (s0 == 1) {  // column-contiguous: a vector runs down VW rows of one column
+#pragma unroll
+        for (int k = 0; k < V::PASS; ++k) {
+            const int c = line + k * (EW_THREADS / V::TPR), r = lane_v;
+            const Vec16<T> v = ldv(p + (i0 + r) + (j0 + c) * s1, 0);
+#pragma unroll
+            for (int e = 0; e < V::VW; ++e) sm[r + e][c] = v.v[e];
+        }
+    } else {        // row-contiguous: a vector runs along VW columns of one row
+#pragma unroll
+        for (int k = 0; k < V::PASS; ++k) {
+            const int r = line + k * (EW_THREADS / V::TPR), c = lane_v;
+            const Vec16<T> v = ldv(p + (i0 + r) * s0 + (j0 + c), 0);
+#pragma unroll
+            for (int e = 0; e < V::VW; ++e) sm[r][c + e] = v.v[e];
+        }
+    }
+}
+
+template <int OP, int CD, bool FPE>
+__global__ void __launch_bounds__(EW_THREADS)
+k_bin_trv(EwDesc d, uint32_t* flags) {
+    typedef typename DT<CD>::T T;
+    typedef BinOp<OP, CD> Op;
+    typedef typename Op::R R;
+    typedef TrV<T> V;
+    static_assert(sizeof(R) == sizeof(T), "the vector path stores results of the operand width");
+    __shared__ T sa[V::TILE][V::TILE + 1], sb[V::TILE][V::TILE + 1];
+    uint32_t bits = 0;
+    const int64_t tr = d.shape[0] / V::TILE, tc = d.shape[1] / V::TILE;
+    const T* pa = (const T*)d.a.p;
+    const T* pb = (const T*)d.b.p;
+    R* po = (R*)d.o;
+    const bool ocol = d.so[0] == 1;
+    const int tid = threadIdx.x;
+    const int lane_v = (tid % V::TPR) * V::VW, line = tid / V::TPR;
+    for (int64_t t = blockIdx.x; t < tr * tc; t += gridDim.x) {
+        const int64_t i0 = (t / tc) * V::TILE, j0 = (t % tc) * V::TILE;
+        trv_load<T>(sa, pa, d.a.st[0], d.a.st[1], i0, j0);
+        trv_load<T>(sb, pb, d.b.st[0], d.b.st[1], i0, j0);
+        __syncthreads();
+#pragma unroll
+        for (int k = 0; k < V::PASS; ++k) {
+            const int m = line + k * (EW_THREADS / V::TPR);
+            R r[V::VW];
+#pragma unroll
+            for (int e = 0; e < V::VW; ++e) {
+                const int rr = ocol ? lane_v + e : m, cc = ocol ? m : lane_v + e;
+                const T x = sa[rr][cc], y = sb[rr][cc];
+                r[e] = Op::apply(x, y);
+                if constexpr (FPE) bits |= fpe_bits<OP, CD>(x, y, r[e]);
+            }
+            R* dst = ocol ? po + (i0 + lane_v) + (j0 + m) * d.so[1] : po + (i0 + m) * d.so[0] + (j0 + lane_v);
+            stv<R, V::VW>(dst, 0, r);
         }
         __syncthreads();
     }
@@ -280,20 +410,21 @@ k_un_nd(EwDesc d, uint32_t* flags) {
     const bool has_m = d.m.p != nullptr;
     if (nd == 1 && !has_m && d.a.dt == CD && d.odt == Op::OUT_DT) {
         // one strided run in the loop dtype (a step-k slice): typed loads,
-        // four in flight per thread before the arithmetic
+        // U in flight per thread before the arithmetic
+        constexpr int U = sizeof(T) >= 8 ? 4 : 8;
         const T* pa = reinterpret_cast<const T*>(d.a.p);
         R* po = reinterpret_cast<R*>(d.o);
         const int64_t stride = (int64_t)gridDim.x * blockDim.x;
         int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-        for (; i + 3 * stride < d.n; i += 4 * stride) {
-            T x[4];
+        for (; i + (U - 1) * stride < d.n; i += U * stride) {
+            T x[U];
 #pragma unroll
-            for (int u = 0; u < 4; ++u) x[u] = __ldcs(pa + (i + u * stride) * sa);
+            for (int u = 0; u < U; ++u) x[u] = ld_cs(pa + (i + u * stride) * sa);
 #pragma unroll
-            for (int u = 0; u < 4; ++u) {
+            for (int u = 0; u < U; ++u) {
                 const R r = Op::apply(x[u]);
                 if constexpr (FPE) bits |= Op::fpe(x[u]);
-                po[(i + u * stride) * so] = r;
+                st_cs(po + (i + u * stride) * so, r);
             }
         }
         for (; i < d.n; i += stride) {

@@ -19,6 +19,21 @@ template <int OP, int CD> constexpr bool bin_valid() {
     return false;
 }
 
+// Whether the vector tile kernel applies: whole tiles, every array either
+// row- or column-contiguous with its other stride and its base a multiple of
+// 16 bytes (so each vector a tile row starts is aligned).
+template <class T> inline bool trv_ok(const EwDesc& d) {
+    constexpr int TL = TrV<T>::TILE, VW = TrV<T>::VW;
+    if (d.shape[0] % TL || d.shape[1] % TL) return false;
+    auto fits = [&](const void* p, int64_t s0, int64_t s1) {
+        if (reinterpret_cast<uintptr_t>(p) % 16) return false;
+        if (s1 == 1) return s0 > 0 && s0 % VW == 0;
+        if (s0 == 1) return s1 > 0 && s1 % VW == 0;
+        return false;
+    };
+    return fits(d.a.p, d.a.st[0], d.a.st[1]) && fits(d.b.p, d.b.st[0], d.b.st[1]) && fits(d.o, d.so[0], d.so[1]);
+}
+
 template <int OP, int CD>
 cudaError_t launch_bin_t(const EwDesc& d, const ContigInfo& ci, uint32_t* flags, cudaStream_t s) {
     typedef typename DT<CD>::T T;
@@ -46,6 +61,19 @@ cudaError_t launch_bin_t(const EwDesc& d, const ContigInfo& ci, uint32_t* flags,
         auto colc = [](int64_t s0, int64_t s1) { return s0 == 1 && s1 != 1; };
         const bool ca = colc(d.a.st[0], d.a.st[1]), cb = colc(d.b.st[0], d.b.st[1]), co = colc(d.so[0], d.so[1]);
         if (ca != co || cb != co) {
+            if constexpr ((sizeof(T) == 4 || sizeof(T) == 8) && sizeof(R) == sizeof(T)) {
+                if (trv_ok<T>(d)) {
+                    constexpr int TL = TrV<T>::TILE;
+                    const int64_t tiles = (d.shape[0] / TL) * (d.shape[1] / TL);
+                    const int g = (int)(tiles < 148 * 6 ? tiles : 148 * 6);
+                    if constexpr (HAS_FPE) {
+                        if (fpe) { k_bin_trv<OP, CD, true><<<g, EW_THREADS, 0, s>>>(d, flags); count_launch(); return cudaGetLastError(); }
+                    }
+                    k_bin_trv<OP, CD, false><<<g, EW_THREADS, 0, s>>>(d, flags);
+                    count_launch();
+                    return cudaGetLastError();
+                }
+            }
             const int64_t tiles = ((d.shape[0] + TR_TILE - 1) / TR_TILE) * ((d.shape[1] + TR_TILE - 1) / TR_TILE);
             const int g = (int)(tiles < 148 * 8 ? tiles : 148 * 8);
             if constexpr (HAS_FPE) {
@@ -55,6 +83,16 @@ cudaError_t launch_bin_t(const EwDesc& d, const ContigInfo& ci, uint32_t* flags,
             count_launch();
             return cudaGetLastError();
         }
+    }
+    if (same && d.nd == 1) {
+        constexpr int U = sizeof(T) >= 8 ? 4 : 8;
+        const int g = ew_grid((d.n + U - 1) / U);
+        if constexpr (HAS_FPE) {
+            if (fpe) { k_bin_run<OP, CD, true><<<g, EW_THREADS, 0, s>>>(d, flags); count_launch(); return cudaGetLastError(); }
+        }
+        k_bin_run<OP, CD, false><<<g, EW_THREADS, 0, s>>>(d, flags);
+        count_launch();
+        return cudaGetLastError();
     }
     int64_t inner = d.shape[d.nd - 1];
     int g = ew_grid(inner >= 64 ? (d.n + 3) / 4 : d.n);

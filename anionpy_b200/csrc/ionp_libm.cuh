@@ -162,16 +162,15 @@ LM_FN float log32(float x) {
 // n and the remainder from 96 bits of 2/pi in integer arithmetic. The
 // quadrant picks the sin or cos polynomial and its sign. (s_sinf.c,
 // sincosf.h)
+// sin (n even) or cos (n odd) polynomial of the reduced argument; both are
+// evaluated and one selected, so lanes of a warp in different quadrants run
+// one body. flip negates the cos polynomial (the table's second half).
 LM_FN float sin32_poly(double x, double x2, int n, bool flip) {
     const double S1 = -0x1.555545995a603p-3, S2 = 0x1.1107605230bc4p-7, S3 = -0x1.994eb3774cf24p-13;
-    if ((n & 1) == 0) {
-        const double x3 = x * x2;
-        const double s1 = fmad(x2, S3, S2);
-        const double x7 = x3 * x2;
-        const double s = fmad(x3, S1, x);
-        return (float)fmad(x7, s1, s);
-    }
-    // cos polynomial; the second half of the quadrants negates it
+    const double x3 = x * x2;
+    const double s1 = fmad(x2, S3, S2);
+    const double x7 = x3 * x2;
+    const double sp = fmad(x7, s1, fmad(x3, S1, x));
     const double sg = flip ? -1.0 : 1.0;
     const double C0 = sg * 0x1p0, C1 = sg * -0x1.ffffffd0c621cp-2, C2 = sg * 0x1.55553e1068f19p-5,
                  C3 = sg * -0x1.6c087e89a359dp-10, C4 = sg * 0x1.99343027bf8c3p-16;
@@ -179,8 +178,8 @@ LM_FN float sin32_poly(double x, double x2, int n, bool flip) {
     const double c2 = fmad(x2, C4, C3);
     const double c1 = fmad(x2, C1, C0);
     const double x6 = x4 * x2;
-    const double c = fmad(x4, C2, c1);
-    return (float)fmad(x6, c2, c);
+    const double cp = fmad(x6, c2, fmad(x4, C2, c1));
+    return (float)((n & 1) ? cp : sp);
 }
 LM_SLOW double sin32_reduce_large(uint32_t xi, int* np) {
     const unsigned int* w = &TWO_OVER_PI_W[(xi >> 26) & 15];
@@ -199,27 +198,25 @@ LM_SLOW double sin32_reduce_large(uint32_t xi, int* np) {
 LM_FN float sin32(float y) {
     const uint32_t ux = fbits(y);
     const uint32_t top = (ux >> 20) & 0x7ff;
-    double x = (double)y;
-    if (top < 0x3f4) {                         // |y| < pi/4 (0x1.921fb6p-1)
-        if (top < 0x398) return y;             // |y| < 2^-12
-        return sin32_poly(x, x * x, 0, false);
+    if (top >= 0x42f) {                        // |y| >= 120, inf, NaN
+        if (top >= 0x7f8) return (ux & 0x7FFFFFu) ? quiet32(y) : dnan32();
+        int n;
+        const int sign = (int)(ux >> 31);
+        const double x = sin32_reduce_large(ux, &n);
+        const int q = n + sign;
+        const double s = ((q + 1) & 2) ? -1.0 : 1.0;   // signs {1,-1,-1,1}[q & 3]
+        return sin32_poly(x * s, x * x, n, (q & 2) != 0);
     }
-    int n;
-    if (top < 0x42f) {                         // |y| < 120
+    double x = (double)y;
+    int n = 0;
+    if (top >= 0x3f4) {                        // pi/4 <= |y| < 120: x - n pi/2
         const double r = x * 0x1.45F306DC9C883p+23;   // x * 2/pi * 2^24
         n = ((int32_t)r + 0x800000) >> 24;
         x = fmad(-(double)n, 0x1.921FB54442D18p0, x);
-        const double s = ((n + 1) & 2) ? -1.0 : 1.0;  // signs {1,-1,-1,1}[n & 3]
-        return sin32_poly(x * s, x * x, n, (n & 2) != 0);
     }
-    if (top < 0x7f8) {
-        const int sign = (int)(ux >> 31);
-        x = sin32_reduce_large(ux, &n);
-        const int q = n + sign;
-        const double s = ((q + 1) & 2) ? -1.0 : 1.0;
-        return sin32_poly(x * s, x * x, n, (q & 2) != 0);
-    }
-    return (ux & 0x7FFFFFu) ? quiet32(y) : dnan32();
+    const double s = ((n + 1) & 2) ? -1.0 : 1.0;
+    const float r = sin32_poly(x * s, x * x, n, (n & 2) != 0);
+    return top < 0x398 ? y : r;                // |y| < 2^-12: y itself
 }
 
 // ------------------------------------------------------------------ exp64
@@ -352,38 +349,36 @@ LM_FN double sin64_taylor(double xx, double a, double da) {
 #define LM_CS4 -4.16666666666664434524222570944589E-02
 #define LM_CS6 1.38888874007937613028114285595617E-03
 
-// cos(x + dx) = cos(X_i) cos(d) - sin(X_i) sin(d), X_i = i/128 nearest |x|
-LM_FN double cos64_tab(double x, double dx) {
-    if (x < 0) dx = -dx;
-    const double u = LM_BIG + fabs(x);
-    x = (fabs(x) - (u - LM_BIG)) + dx;
-    const double xx = x * x;
-    const double s = fmad(x * xx, fmad(xx, LM_SN5, LM_SN3), x);
-    const double c = xx * fmad(xx, fmad(xx, LM_CS6, LM_CS4), LM_CS2);
-    const int k = (int)(uint32_t)dbits(u) << 2;
-    const double sn = ld(&SINCOS_TAB[k]), ssn = ld(&SINCOS_TAB[k + 1]);
-    const double cs = ld(&SINCOS_TAB[k + 2]), ccs = ld(&SINCOS_TAB[k + 3]);
-    const double cor = fmad(-sn, s, fmad(-cs, c, fmad(-s, ssn, ccs)));
-    return cs + cor;
-}
-// sin(x + dx): Taylor below 0.126, else sin(X_i) cos(d) + cos(X_i) sin(d)
-LM_FN double sin64_tab(double x, double dx) {
-    const double x0 = x;
-    if (fabs(x) < 0.126) return sin64_taylor(x * x, x, dx);
-    if (x <= 0) dx = -dx;
-    const double u = LM_BIG + fabs(x);
-    x = fabs(x) - (u - LM_BIG);
-    const double xx = x * x;
-    const double s = x + fmad(x * xx, fmad(xx, LM_SN5, LM_SN3), dx);
-    const double c = fmad(x, dx, xx * fmad(xx, fmad(xx, LM_CS6, LM_CS4), LM_CS2));
-    const int k = (int)(uint32_t)dbits(u) << 2;
-    const double sn = ld(&SINCOS_TAB[k]), ssn = ld(&SINCOS_TAB[k + 1]);
-    const double cs = ld(&SINCOS_TAB[k + 2]), ccs = ld(&SINCOS_TAB[k + 3]);
-    const double cor = fmad(cs, s, fmad(-sn, c, fmad(s, ccs, ssn)));
-    return copysign(sn + cor, x0);
-}
+// sin or cos of a + da (|a| < 0.86) from the table of i/128, evaluated
+// without a branch on which: both of glibc's correction formulas are
+// computed and one is selected (a warp whose lanes need different ones runs
+// one body). With n even: sin(a + da), as s_sin.c's do_sin (Taylor series
+// below |a| = 0.126; else sin(X_i) cos(d) + cos(X_i) sin(d), X_i = i/128
+// nearest |a|). With n odd: cos(a + da), as do_cos (cos(X_i) cos(d) -
+// sin(X_i) sin(d)). n & 2 negates the result.
 LM_FN double sin64_quadrant(double a, double da, int n) {
-    const double r = (n & 1) ? cos64_tab(a, da) : sin64_tab(a, da);
+    const bool cosq = (n & 1) != 0;
+    const double dxs = (cosq ? (a < 0) : (a <= 0)) ? -da : da;
+    const double ax = fabs(a);
+    const double u = LM_BIG + ax;
+    const double t = ax - (u - LM_BIG);
+    const double x = cosq ? t + dxs : t;
+    const double xx = x * x;
+    const double ps = fmad(xx, LM_SN5, LM_SN3);
+    const double pc = xx * fmad(xx, fmad(xx, LM_CS6, LM_CS4), LM_CS2);
+    const double s = cosq ? fmad(x * xx, ps, x) : x + fmad(x * xx, ps, dxs);
+    const double c = cosq ? pc : fmad(x, dxs, pc);
+    const int k = (int)(uint32_t)dbits(u) << 2;
+    const double sn = ld(&SINCOS_TAB[k]), ssn = ld(&SINCOS_TAB[k + 1]);
+    const double cs = ld(&SINCOS_TAB[k + 2]), ccs = ld(&SINCOS_TAB[k + 3]);
+    double r;
+    if (cosq) {
+        r = cs + fmad(-sn, s, fmad(-cs, c, fmad(-s, ssn, ccs)));
+    } else if (ax < 0.126) {
+        r = sin64_taylor(a * a, a, da);
+    } else {
+        r = copysign(sn + fmad(cs, s, fmad(-sn, c, fmad(s, ccs, ssn))), a);
+    }
     return (n & 2) ? -r : r;
 }
 // |x| >= 105414350: x 2/pi = sum + b + bb from 24-bit chunks of 2/pi, each
@@ -450,24 +445,27 @@ LM_SLOW double sin64_large(double x) {
 LM_FN double sin64(double x) {
     const uint32_t k = (uint32_t)(dbits(x) >> 32) & 0x7fffffffu;
     if (k < 0x3e500000u) return x;                       // |x| < 2^-26
-    if (k < 0x3feb6000u) return sin64_tab(x, 0.0);       // |x| < 0.855469
-    if (k < 0x400368fdu) {                               // |x| < 2.426265
-        const double t = LM_HP0 - fabs(x);
-        return copysign(cos64_tab(t, LM_HP1), x);
+    if (k >= 0x419921fbu) {                              // |x| >= 105414350, inf, NaN
+        if (k < 0x7ff00000u) return sin64_large(x);
+        return ((dbits(x) << 12) != 0) ? quiet64(x) : dnan64();
     }
-    if (k < 0x419921fbu) {                               // |x| < 105414350
+    double a, da;
+    int n;
+    if (k < 0x3feb6000u) {                               // |x| < 0.855469: sin(x)
+        a = x; da = 0.0; n = 0;
+    } else if (k < 0x400368fdu) {                        // |x| < 2.426265: +-cos(pi/2 - |x|)
+        a = LM_HP0 - fabs(x); da = LM_HP1; n = x < 0 ? 3 : 1;
+    } else {                                             // Cody-Waite: x - n pi/2 in four parts
         const double t = fmad(x, 0x1.45f306dc9c883p-1, 0x1.8p52);   // x 2/pi + shifter
         const double xn = t - 0x1.8p52;
         const double y = fmad(-xn, LM_MP2, fmad(-xn, LM_MP1, x));
-        const int n = (int)(dbits(t) & 3);
+        n = (int)(dbits(t) & 3);
         const double t2 = fmad(-xn, LM_PP3, y);
-        double db = fmad(-xn, LM_PP3, y - t2);
-        const double b = fmad(-xn, LM_PP4, t2);
-        db += fmad(-xn, LM_PP4, t2 - b);
-        return sin64_quadrant(b, db, n);
+        da = fmad(-xn, LM_PP3, y - t2);
+        a = fmad(-xn, LM_PP4, t2);
+        da += fmad(-xn, LM_PP4, t2 - a);
     }
-    if (k < 0x7ff00000u) return sin64_large(x);
-    return ((dbits(x) << 12) != 0) ? quiet64(x) : dnan64();
+    return sin64_quadrant(a, da, n);
 }
 
 }  // namespace lm

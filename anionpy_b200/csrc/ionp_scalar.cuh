@@ -461,8 +461,36 @@ template <class I> __device__ __forceinline__ I w_mul(I x, I y) {
     if constexpr (sizeof(I) < 4) return (I)(U)((uint32_t)(U)x * (uint32_t)(U)y);
     else return (I)(U)((U)x * (U)y);
 }
+// Truncated quotient of 64-bit magnitudes (uy != 0). A 64-bit division is a
+// long emulated sequence on the GPU; this one needs it only for quotients of
+// 2^20 or more. Below that, fq = rz(rz(ux) * rcp_rz(ru(uy))) never exceeds
+// ux / uy (every rounding is toward it) and is within a relative 2^-21 of
+// it, so trunc(fq) is the exact quotient or at most one or two below; the
+// remainder ux - q uy (no underflow: q uy <= ux) then repairs q exactly.
+__device__ __forceinline__ uint64_t udiv64_trunc(uint64_t ux, uint64_t uy) {
+    if (ux < uy) return 0;
+    const float fq = __fmul_rz(__ull2float_rz(ux), __frcp_rz(__ull2float_ru(uy)));
+    if (fq < 0x1p20f) {
+        uint64_t q = (uint64_t)fq;
+        uint64_t r = ux - q * uy;
+        if (r >= uy) { ++q; r -= uy; }
+        if (r >= uy) ++q;
+        return q;
+    }
+    return ux / uy;
+}
 template <class I> __device__ __forceinline__ I w_div(I x, I y) {
     if constexpr (std::is_signed<I>::value) { if (y == (I)-1) return w_sub<I>((I)0, x); }
+    if constexpr (sizeof(I) == 8) {
+        if constexpr (std::is_signed<I>::value) {
+            const uint64_t ux = x < 0 ? 0ull - (uint64_t)x : (uint64_t)x;
+            const uint64_t uy = y < 0 ? 0ull - (uint64_t)y : (uint64_t)y;
+            const uint64_t q = udiv64_trunc(ux, uy);
+            return (I)(((x < 0) != (y < 0)) ? 0ull - q : q);
+        } else {
+            return (I)udiv64_trunc((uint64_t)x, (uint64_t)y);
+        }
+    }
     return (I)(x / y);
 }
 template <class I> __device__ __forceinline__ I w_rem(I x, I y) {

@@ -259,3 +259,69 @@ def test_float_floor_divide_quotient_edges(dt):
     got = ap.floor_divide(ap.from_numpy(xs), ap.from_numpy(ys)).get()
     want, _ = O.binary("floor_divide", xs, ys)
     assert_bits_equal(got, want, f"floor_divide {np.dtype(dt).name} quotient edges")
+
+
+@pytest.mark.parametrize("dt", [np.float32, np.int32, np.uint32, np.float64, np.int64], ids=lambda d: np.dtype(d).name)
+@pytest.mark.parametrize("shape", [(64, 64), (128, 192), (320, 64)])
+def test_transposed_whole_vector_tiles(dt, shape):
+    """Whole 64 x 64 (4-byte) or 32 x 32 (8-byte) tiles with 16-byte aligned
+    rows: the vector tile kernel, both output layouts, FPE categories; a view
+    whose rows start off a 16-byte boundary takes the scalar tile kernel and
+    must give the same bits."""
+    rng = np.random.default_rng(21)
+    base = array(dt, shape[::-1], rng, zeros=0.02)
+    w = array(dt, shape, rng, zeros=0.02)
+    ops = ["add", "maximum", "multiply", "subtract", "floor_divide", "remainder"]
+    if np.dtype(dt).kind in "iu":
+        ops.append("bitwise_and")
+    db, dw = ap.from_numpy(base), ap.from_numpy(w)
+    for op in ops:
+        want, wcat = O.binary(op, base.T, w)
+        got, cat = run(lambda: getattr(ap, op)(db.T, dw))
+        assert_bits_equal(got.get(), want, f"{op} {shape}")
+        assert cat == wcat, f"{op} {shape}: FPE {cat} != {wcat}"
+        for order in ("C", "F"):
+            dout = ap.from_numpy(np.zeros(shape, want.dtype, order=order))
+            getattr(ap, op)(db.T, dw, out=dout)
+            assert_bits_equal(dout.get(), want, f"{op} {shape} out={order}")
+    # rows starting one element past a 16-byte boundary
+    big = array(dt, (shape[1] + 1, shape[0] + 1), rng)
+    v = big[1:, 1:]
+    want = O.binary("add", v.T, w)[0]
+    got = ap.add(ap.from_numpy(big)[1:, 1:].T, dw)
+    assert_bits_equal(got.get(), want, f"misaligned {shape}")
+
+
+@pytest.mark.parametrize("dt", [np.int64, np.uint64], ids=lambda d: np.dtype(d).name)
+def test_int64_division_quotient_ranges(dt):
+    """floor_divide / remainder on 64-bit integers: full-range operands (small
+    quotients), quotients around the 2^20 limit of the estimate path, huge
+    quotients (the exact division), the extremes and zero divisors, each
+    contiguous and through a step-2 slice."""
+    rng = np.random.default_rng(33)
+    info = np.iinfo(dt)
+    n = 1 << 16
+    y = rng.integers(1, 1 << 40, n, dtype=np.int64).astype(dt)
+    q = rng.integers((1 << 20) - 4, (1 << 20) + 4, n).astype(dt)
+    with np.errstate(all="ignore"):
+        near = (q * y + rng.integers(0, 1 << 30, n).astype(dt) % y).astype(dt)
+    parts_x = [rng.integers(info.min, info.max, n, dtype=dt, endpoint=True), near,
+               rng.integers(info.min, info.max, n, dtype=dt, endpoint=True)]
+    parts_y = [rng.integers(info.min, info.max, n, dtype=dt, endpoint=True), y,
+               rng.integers(1, 1000, n).astype(dt)]
+    ext = np.array([info.min, info.max, 0, 1, 2, info.max - 1, info.min + 1] + ([-1, -2] if dt == np.int64 else [3, 7]), dt)
+    ex_x, ex_y = np.meshgrid(ext, ext)
+    x = np.concatenate(parts_x + [ex_x.ravel()])
+    yy = np.concatenate(parts_y + [ex_y.ravel()])
+    if dt == np.int64:
+        x[: n // 2] = -np.abs(x[: n // 2] // 2)
+        yy[n: n + n // 2] = -yy[n: n + n // 2]
+        x[2 * n + n // 3: 2 * n + n // 2] *= -1
+    for op in ("floor_divide", "remainder"):
+        want, wcat = O.binary(op, x, yy)
+        got, cat = run(lambda: getattr(ap, op)(ap.from_numpy(x), ap.from_numpy(yy)))
+        assert_bits_equal(got.get(), want, f"{op} contiguous")
+        assert cat == wcat
+        x2, y2 = np.repeat(x, 2), np.repeat(yy, 2)
+        got2 = getattr(ap, op)(ap.from_numpy(x2)[::2], ap.from_numpy(y2)[::2])
+        assert_bits_equal(got2.get(), want, f"{op} step-2")
