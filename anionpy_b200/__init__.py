@@ -1,8 +1,9 @@
 """anionpy_b200 -- anionpy's ufunc-engine hot path on NVIDIA B200.
 
 Drop-in for the element-wise ufunc ``__call__`` (unary and binary, with
-broadcasting and arbitrary strides), ``ufunc.reduce`` and ``argmin``/
-``argmax`` of anionpy, computed by hand-written sm_100a CUDA kernels behind the
+broadcasting and arbitrary strides), ``ufunc.reduce``, ``argmin``/``argmax``
+and the reductions built on them (``sum``, ``prod``, ``min``, ``max``,
+``any``, ``all``, ``mean``, also as array methods) of anionpy, computed by hand-written sm_100a CUDA kernels behind the
 C ABI of ``libionp_cuda.so`` (include/ionp_cuda.h). Results are bit-exact with
 anionpy's CPU path; errors and ``errstate`` behave the same way.
 """
@@ -15,9 +16,11 @@ from ._ufunc import (BINARY_OPS, UNARY_OPS, absolute, add, argmax, argmin, bitwi
                      less, less_equal, log, logical_and, logical_not, logical_or, logical_xor, maximum, minimum, mod,
                      multiply, negative, not_equal, remainder, right_shift, sin, sqrt, subtract, true_divide, ufunc)
 from ._ufunc import abs  # noqa: A001
+from ._reductions import all, amax, amin, any, max, mean, min, prod, sum  # noqa: A004
 
 __all__ = [
     "ndarray", "array", "asarray", "empty", "zeros", "ones", "from_numpy",
     "errstate", "seterr", "geterr", "seterrcall", "geterrcall", "AxisError", "UFuncTypeError",
     "ufunc", "argmax", "argmin", "launch_count", "Batch",
+    "sum", "prod", "min", "max", "amin", "amax", "any", "all", "mean",
 ] + list(BINARY_OPS) + list(UNARY_OPS) + ["true_divide", "mod", "abs", "bitwise_not"]

@@ -250,14 +250,74 @@ class ndarray:
             check(lib().ionp_cast(ctypes.byref(self._desc()), ctypes.byref(out._desc()), None))
         return out
 
-    def astype(self, dtype, copy=True):
+    def astype(self, dtype, order="K", casting="unsafe", subok=True, copy=True):
+        """ndarray.astype (ionp-py/src/lib.rs:5960-6003): the casting= rule
+        check, detect_cast_overflow (a float source cast to an integer
+        dtype: NaN, infinity or out-of-range values report "invalid value
+        encountered in cast" through errstate), then the cast."""
+        from . import _fpstate
+        from ._lib import CAST_RULES
+        from ._ufunc import _can_cast
         dt = np.dtype(dtype)
+        if casting not in CAST_RULES:
+            raise ValueError("casting must be one of 'no', 'equiv', 'safe', 'same_kind', or 'unsafe'")
+        if not _can_cast(self._dtype, dt, CAST_RULES[casting]):
+            raise TypeError(f"Cannot cast array data from {self._dtype!r} to {dt!r} according to the rule '{casting}'")
         if dt == self._dtype and not copy:
             return self
+        out = ndarray.empty(self._shape, dt)
+        fpe = ctypes.c_uint32(0)
+        check(lib().ionp_astype(ctypes.byref(self._desc()), ctypes.byref(out._desc()), ctypes.byref(fpe), None))
+        if fpe.value & 8:
+            _fpstate.signal("invalid", "cast", stacklevel=3)
+        return out
+
+    def _cast_to(self, dtype):
+        """Buffer::cast_to (ionp-core/src/buffer.rs:210): a C-ordered copy in
+        dtype, with no FPE check (the reference's internal casts)."""
+        dt = np.dtype(dtype)
         out = ndarray.empty(self._shape, dt)
         if self.size:
             check(lib().ionp_cast(ctypes.byref(self._desc()), ctypes.byref(out._desc()), None))
         return out
+
+    # ---- reductions (ndarray_attrs.rs:675-760: the same functions as
+    # anionpy.sum etc., reached as methods) --------------------------------
+    def sum(self, axis=None, dtype=None, out=None, keepdims=None, initial=None, where=None):
+        from . import _reductions
+        return _reductions.sum(self, axis, dtype, out, keepdims, initial, where)
+
+    def prod(self, axis=None, dtype=None, out=None, keepdims=None, initial=None, where=None):
+        from . import _reductions
+        return _reductions.prod(self, axis, dtype, out, keepdims, initial, where)
+
+    def min(self, axis=None, out=None, keepdims=None, initial=None, where=None):
+        from . import _reductions
+        return _reductions.min(self, axis, out, keepdims, initial, where)
+
+    def max(self, axis=None, out=None, keepdims=None, initial=None, where=None):
+        from . import _reductions
+        return _reductions.max(self, axis, out, keepdims, initial, where)
+
+    def all(self, axis=None, out=None, keepdims=None, where=None):
+        from . import _reductions
+        return _reductions.all(self, axis, out, keepdims, where)
+
+    def any(self, axis=None, out=None, keepdims=None, where=None):
+        from . import _reductions
+        return _reductions.any(self, axis, out, keepdims, where)
+
+    def mean(self, axis=None, dtype=None, out=None, keepdims=None, where=None):
+        from . import _reductions
+        return _reductions.mean(self, axis, dtype, out, keepdims, where)
+
+    def argmax(self, axis=None, out=None, keepdims=False):
+        from . import _ufunc
+        return _ufunc.argmax(self, axis, out, keepdims)
+
+    def argmin(self, axis=None, out=None, keepdims=False):
+        from . import _ufunc
+        return _ufunc.argmin(self, axis, out, keepdims)
 
     # ---- operators (thin wrappers over the ufuncs) -----------------------
     def _uf(name):

@@ -25,7 +25,7 @@ CAST_RULES = {"no": 0, "equiv": 1, "safe": 2, "same_kind": 3, "unsafe": 4}
 
 # status codes
 OK, ERR_BROADCAST, ERR_TYPE, ERR_VALUE, ERR_NO_LOOP, ERR_AXIS, ERR_CUDA, ERR_TIMEOUT, ERR_OOM, \
-    ERR_UNSUPPORTED, ERR_INVALID = range(11)
+    ERR_UNSUPPORTED, ERR_INVALID, ERR_INDEX = range(12)
 
 FPE_DIVIDE, FPE_OVER, FPE_UNDER, FPE_INVALID = 1, 2, 4, 8
 
@@ -69,8 +69,12 @@ _SIGS = {
     "ionp_binary_nowait": [ctypes.c_int32, _P, _P, _P, _P, ctypes.c_void_p, ctypes.c_void_p],
     "ionp_unary_nowait": [ctypes.c_int32, _P, _P, _P, ctypes.c_void_p, ctypes.c_void_p],
     "ionp_cast": [_P, _P, ctypes.c_void_p],
+    "ionp_astype": [_P, _P, ctypes.POINTER(ctypes.c_uint32), ctypes.c_void_p],
     "ionp_reduce": [ctypes.c_int32, _P, ctypes.POINTER(ctypes.c_int32), ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
                     ctypes.c_void_p, _P, _P, ctypes.c_void_p],
+    "ionp_accumulate": [ctypes.c_int32, _P, ctypes.c_int32, _P, ctypes.c_void_p],
+    "ionp_reduceat": [ctypes.c_int32, _P, ctypes.c_int32, ctypes.POINTER(ctypes.c_int64), ctypes.c_int64, _P,
+                      ctypes.c_void_p],
     "ionp_argext": [ctypes.c_int32, _P, ctypes.c_int32, ctypes.c_int32, _P, ctypes.c_void_p],
     "ionp_alloc": [ctypes.POINTER(ctypes.c_void_p), ctypes.c_size_t, ctypes.c_void_p],
     "ionp_free": [ctypes.c_void_p, ctypes.c_void_p],
@@ -185,6 +189,8 @@ def check(status: int):
         raise TimeoutError(msg)
     if status == ERR_UNSUPPORTED:
         raise TypeError(msg)
+    if status == ERR_INDEX:
+        raise IndexError(msg)
     raise RuntimeError(f"CUDA failure: {msg}")
 
 

@@ -173,7 +173,7 @@ class ufunc:
                 for i, o in enumerate(ops):
                     if not _can_cast(o.dtype, dt, rule):
                         raise UFuncTypeError(f"Cannot cast ufunc '{self.__name__}' input {i} from {o.dtype!r} to {dt!r} with casting rule '{casting}'")
-                    cast.append(o if o.dtype == dt else o.astype(dt))
+                    cast.append(o if o.dtype == dt else o._cast_to(dt))
                 ops = cast
         elif rule <= 1:
             # casting='no'/'equiv' without dtype=: the loop dtype must equal the inputs
@@ -238,6 +238,15 @@ class ufunc:
 
     # ---- reduce ------------------------------------------------------------
     def reduce(self, array, axis=0, dtype=None, out=None, keepdims=False, initial=_NOVALUE, where=True):
+        res = self._reduce_nd(array, axis, dtype, out, keepdims, initial, where)
+        if out is not None:
+            return res
+        if res.ndim == 0:
+            return _scalar_result(res)
+        return res
+
+    def _reduce_nd(self, array, axis=0, dtype=None, out=None, keepdims=False, initial=_NOVALUE, where=True):
+        """ufunc.reduce returning the device array (0-d included)."""
         if self.nin != 2:
             raise ValueError("reduce only supported for binary functions")
         a = array if isinstance(array, ndarray) else asarray(array)
@@ -286,10 +295,6 @@ class ufunc:
                             code_of(cd) if dtype is not None else -1,
                             init_buf.ctypes.data if init_buf is not None else None,
                             ctypes.byref(md) if md is not None else None, ctypes.byref(res._desc()), None))
-        if out is not None:
-            return out
-        if res.ndim == 0:
-            return _scalar_result(res)
         return res
 
 

@@ -854,6 +854,64 @@ int32_t ionp_cast(const IonpArr* a, IonpArr* out, IonpStream stream) {
     return cast_impl(a, out, nullptr, (cudaStream_t)stream);
 }
 
+// ndarray.astype (ionp-py/src/lib.rs:5960-6003): detect_cast_overflow
+// (fpe.rs:398) on the source, then the cast. Only a float source cast to an
+// integer destination is checked; its bounds are the destination's range as
+// float64 (i64::MAX as f64 is 2^63, so 2^63 itself is not flagged).
+int32_t ionp_astype(const IonpArr* a, IonpArr* out, uint32_t* fpe, IonpStream stream) {
+    int32_t st;
+    if ((st = check_arr(a, "a")) || (st = check_arr(out, "out"))) return st;
+    cudaStream_t s = (cudaStream_t)stream;
+    if (fpe) *fpe = 0;
+    const bool to_int = !dt_is_float(out->dtype) && out->dtype != DT_BOOL;
+    if (fpe && dt_is_float(a->dtype) && to_int && numel(a) > 0) {
+        double lo, hi;
+        switch (out->dtype) {
+            case DT_I8: lo = -128.0; hi = 127.0; break;
+            case DT_I16: lo = -32768.0; hi = 32767.0; break;
+            case DT_I32: lo = -2147483648.0; hi = 2147483647.0; break;
+            case DT_I64: lo = -9223372036854775808.0; hi = 9223372036854775808.0; break;
+            case DT_U8: lo = 0.0; hi = 255.0; break;
+            case DT_U16: lo = 0.0; hi = 65535.0; break;
+            case DT_U32: lo = 0.0; hi = 4294967295.0; break;
+            default: lo = 0.0; hi = 18446744073709551616.0; break;
+        }
+        MergeIn mi;
+        memset(&mi, 0, sizeof(mi));
+        mi.nd = a->ndim;
+        mi.nops = 1;
+        for (int i = 0; i < a->ndim; ++i) { mi.shape[i] = a->shape[i]; mi.st[0][i] = a->strides[i]; }
+        MergeOut mo = merge_dims(mi);
+        FlagWord fw;
+        if ((st = fw.open(s))) return st;
+        const int lead = mo.nd > EW_MAXD ? mo.nd - EW_MAXD : 0;
+        int64_t nlead = 1;
+        for (int i = 0; i < lead; ++i) nlead *= mo.shape[i];
+        for (int64_t q = 0; q < nlead; ++q) {
+            int64_t rem = q, oa = 0;
+            for (int i = lead - 1; i >= 0; --i) {
+                oa += (rem % mo.shape[i]) * mo.st[0][i];
+                rem /= mo.shape[i];
+            }
+            EwDesc d;
+            memset(&d, 0, sizeof(d));
+            d.nd = mo.nd - lead;
+            d.n = 1;
+            for (int i = 0; i < d.nd; ++i) {
+                d.shape[i] = mo.shape[lead + i];
+                d.n *= d.shape[i];
+                d.a.st[i] = mo.st[0][lead + i];
+            }
+            if (d.nd == 0) { d.nd = 1; d.shape[0] = 1; d.n = 1; }
+            d.a.p = elem_ptr(a) + oa * dt_bytes(a->dtype);
+            d.a.dt = a->dtype;
+            if ((st = cuda_err(launch_cast_check(d, lo, hi, fw.d, s), "cast overflow detector"))) return st;
+        }
+        if ((st = fw.read(fpe))) return st;
+    }
+    return cast_impl(a, out, nullptr, s);
+}
+
 }  // extern "C"
 
 namespace ionp {

@@ -123,6 +123,39 @@ __global__ void __launch_bounds__(EW_THREADS) k_cast(EwDesc d) {
     }
 }
 
+// detect_cast_overflow (ionp-core/src/fpe.rs:398-424): a float source
+// element that is not finite or lies outside [lo, hi] (the destination
+// integer type's range as float64) sets FPE_INVALID. Every element is
+// widened to float64 first, as the reference's to_f64_lossy does.
+template <int SD>
+__global__ void __launch_bounds__(EW_THREADS) k_cast_check(EwDesc d, double lo, double hi, uint32_t* flags) {
+    typedef typename DT<SD>::T S;
+    bool bad = false;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < d.n; i += stride) {
+        const Offs f = unravel(d, i, 0);
+        const S v = ((const S*)d.a.p)[f.a];
+        double x;
+        if constexpr (SD == DT_F16) x = (double)h2f(v);
+        else x = (double)v;
+        if (!(x >= lo && x <= hi)) bad = true;
+    }
+    flush_flags(bad ? FPE_INVALID : 0u, flags);
+}
+
+cudaError_t launch_cast_check(const EwDesc& d, double lo, double hi, uint32_t* flags, cudaStream_t s) {
+    if (d.n == 0) return cudaSuccess;
+    const int g = ew_grid(d.n);
+    switch (d.a.dt) {
+        case DT_F16: k_cast_check<DT_F16><<<g, EW_THREADS, 0, s>>>(d, lo, hi, flags); break;
+        case DT_F32: k_cast_check<DT_F32><<<g, EW_THREADS, 0, s>>>(d, lo, hi, flags); break;
+        case DT_F64: k_cast_check<DT_F64><<<g, EW_THREADS, 0, s>>>(d, lo, hi, flags); break;
+        default: return cudaErrorInvalidValue;
+    }
+    count_launch();
+    return cudaGetLastError();
+}
+
 cudaError_t launch_cast(const EwDesc& d, cudaStream_t s) {
     // (k_cast<DD> is instantiated for all 12 output dtypes by design)
     if (d.n == 0) return cudaSuccess;

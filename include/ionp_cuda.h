@@ -63,7 +63,8 @@ enum {
     IONP_ERR_TIMEOUT = 7,     /* a bounded device-side wait ran out */
     IONP_ERR_OOM = 8,         /* device allocation failed */
     IONP_ERR_UNSUPPORTED = 9, /* dtype/op outside this engine (e.g. complex) */
-    IONP_ERR_INVALID = 10     /* malformed descriptor or argument */
+    IONP_ERR_INVALID = 10,    /* malformed descriptor or argument */
+    IONP_ERR_INDEX = 11       /* IonpError::Index      -> IndexError */
 };
 
 /* FPE category bits (ionp-core/src/fpe.rs:43-48) */
@@ -138,6 +139,12 @@ int32_t ionp_unary_nowait(int32_t op, const IonpArr* a, IonpArr* out, const Ionp
 /* Element-wise dtype conversion/copy of `a` into `out` (same shape, any
  * strides): Buffer::cast_to (ionp-core/src/buffer.rs:210). */
 int32_t ionp_cast(const IonpArr* a, IonpArr* out, IonpStream stream);
+/* ndarray.astype (ionp-py/src/lib.rs:5960-6003): the cast above preceded
+ * by detect_cast_overflow (ionp-core/src/fpe.rs:398). fpe (NULL, or a host
+ * word) receives IONP_FPE_INVALID when a float source holds a NaN, an
+ * infinity or a value outside the integer destination's range; other
+ * casts never flag. A non-NULL fpe makes the call wait for the stream. */
+int32_t ionp_astype(const IonpArr* a, IonpArr* out, uint32_t* fpe, IonpStream stream);
 /* ufunc.reduce: reduce_axis (ufunc.rs:7634).
  *   axes          : normalized, sorted, unique (normalize_reduce_axes, ufunc.rs:7551)
  *   compute_dtype : -1 = reduce_family_compute_dtype, else the dtype= override
@@ -182,6 +189,18 @@ int32_t ionp_reduce(int32_t op, const IonpArr* a, const int32_t* axes, int32_t n
 #define IONP_NOALLOC_SCRATCH_BYTES (1u << 20)
 int32_t ionp_reduce_noalloc(int32_t op, const IonpArr* a, const int32_t* axes, int32_t naxes, int32_t keepdims,
                             const void* initial, IonpArr* out, IonpStream stream);
+/* ufunc.accumulate / cumsum / cumprod: accumulate_axis (ufunc.rs:7967):
+ * every fiber along `axis` (0 <= axis < ndim) folded in order, acc = x0,
+ * acc = op(acc, x_i), in reduce_family_compute_dtype (ufunc.rs:2080).
+ * out: a's shape, any strides, cast on store. */
+int32_t ionp_accumulate(int32_t op, const IonpArr* a, int32_t axis, IonpArr* out, IonpStream stream);
+/* ufunc.reduceat: reduceat_binary_axis (ufunc.rs:8450): segment k of every
+ * fiber is x[indices[k]] .. x[indices[k+1] - 1] (to the axis end for the
+ * last), folded in order, or x[indices[k]] alone when indices[k+1] <=
+ * indices[k]. indices: HOST int64 array, each in [0, a.shape[axis]), else
+ * IONP_ERR_INDEX. out: a's shape with the axis extent nindices. */
+int32_t ionp_reduceat(int32_t op, const IonpArr* a, int32_t axis, const int64_t* indices, int64_t nindices,
+                      IonpArr* out, IonpStream stream);
 /* argmin (is_max=0) / argmax (is_max=1): argext (ufunc.rs:8131) behind
  * do_argext (ionp-py/src/reductions.rs:1198). axis = -1 means the flattened
  * C-order ravel (axis=None); out is int64 with the kept shape. */

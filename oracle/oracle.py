@@ -335,3 +335,44 @@ def reduce_layout_strides(shape, strides, axes, keepdims):
     if int(np.prod(pretend)) == 0:
         full_st = [0] * nd
     return full_st
+
+
+def mean(a: np.ndarray, axis=None, dtype=None, keepdims=False, where=None):
+    """numpy's mean as the reference composes it (ionp-py/src/reductions.rs:
+    1515-1734): (values, warned_empty, fpe category of the internal divide).
+    Sum with add.reduce (float16 results sum in float32, bool/int input in
+    float64 unless dtype= says otherwise), divide in float64 for float16 and
+    float32 sums, cast back once; where= divides by the mask's count."""
+    a = np.asarray(a)
+    axes = normalize_reduce_axes(axis, a.ndim)
+    over = None if dtype is None else np.dtype(dtype)
+    default = np.dtype(np.float64) if over is None and (a.dtype == np.bool_ or a.dtype.kind in "iu") else over
+    effective = default if default is not None else a.dtype
+    f16_widen = effective == np.float16
+    sum_cd = np.dtype(np.float32) if f16_widen else default
+    mask = None if where is None else np.broadcast_to(np.asarray(where), a.shape)
+    s = np.asarray(reduce("add", a, axis=tuple(axes), dtype=sum_cd, keepdims=False,
+                          where=None if mask is None else mask))
+    out_dt = s.dtype
+    div_dt = np.dtype(np.float64) if out_dt in (np.float16, np.float32) else out_dt
+    if mask is not None:
+        count = np.asarray(reduce("add", cast(np.ascontiguousarray(mask), np.int64), axis=tuple(axes), keepdims=False))
+    else:
+        n = 1
+        for ax in axes:
+            n *= a.shape[ax]
+        count = np.array(n, np.int64)
+    cnt = cast(np.asarray(count), div_dt)
+    num = cast(s, div_dt) if div_dt != out_dt else s
+    warned = bool(np.any(cnt == 0))
+    raw, cat = binary("divide", num, cnt)
+    res = raw
+    if div_dt != out_dt:
+        res = cast(res, out_dt)
+    if f16_widen:
+        res = cast(res, np.float16)
+    elif res.dtype != effective:
+        res = cast(res, effective)
+    if keepdims:
+        res = res.reshape([1 if i in axes else a.shape[i] for i in range(a.ndim)])
+    return res, warned, cat

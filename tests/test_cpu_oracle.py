@@ -170,3 +170,22 @@ def test_transcendentals_are_glibc_and_within_one_ulp_of_correct_rounding():
     ld = np.exp(x.astype(np.longdouble))
     err = np.abs((got.astype(np.longdouble) - ld) / np.spacing(got)).max()
     assert err <= 1.0
+
+
+def test_oracle_mean_matches_numpy():
+    """The oracle's mean (the reference's composition, reductions.rs:1515)
+    equals NumPy's bit for bit on C-ordered inputs, which the reference
+    declares; float16 sums in float32, float32 divides in float64."""
+    rng = np.random.default_rng(1)
+    for dt in (np.float16, np.float32, np.float64, np.int8, np.int32, np.int64, np.uint16, np.bool_):
+        if np.dtype(dt).kind == "f":
+            a = rng.standard_normal((6, 7, 8)).astype(dt)
+        elif dt == np.bool_:
+            a = rng.random((6, 7, 8)) < 0.5
+        else:
+            a = rng.integers(-100 if np.dtype(dt).kind == "i" else 0, 100, (6, 7, 8)).astype(dt)
+        for kw in ({}, {"axis": 0}, {"axis": -1}, {"axis": (0, 2)}, {"axis": 1, "keepdims": True},
+                   {"axis": 1, "dtype": np.float32}):
+            got = O.mean(a, **kw)[0]
+            want = np.asarray(np.mean(a, **kw))
+            assert got.dtype == want.dtype and got.tobytes() == want.tobytes(), (np.dtype(dt).name, kw)
