@@ -16,11 +16,11 @@ from ._ufunc import (BINARY_OPS, UNARY_OPS, absolute, add, argmax, argmin, bitwi
                      less, less_equal, log, logical_and, logical_not, logical_or, logical_xor, maximum, minimum, mod,
                      multiply, negative, not_equal, remainder, right_shift, sin, sqrt, subtract, true_divide, ufunc)
 from ._ufunc import abs  # noqa: A001
-from ._reductions import all, amax, amin, any, max, mean, min, prod, sum  # noqa: A004
+from ._reductions import all, amax, amin, any, cumprod, cumsum, max, mean, min, prod, sum  # noqa: A004
 
 __all__ = [
     "ndarray", "array", "asarray", "empty", "zeros", "ones", "from_numpy",
     "errstate", "seterr", "geterr", "seterrcall", "geterrcall", "AxisError", "UFuncTypeError",
     "ufunc", "argmax", "argmin", "launch_count", "Batch",
-    "sum", "prod", "min", "max", "amin", "amax", "any", "all", "mean",
+    "sum", "prod", "min", "max", "amin", "amax", "any", "all", "mean", "cumsum", "cumprod",
 ] + list(BINARY_OPS) + list(UNARY_OPS) + ["true_divide", "mod", "abs", "bitwise_not"]

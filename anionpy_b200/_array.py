@@ -311,6 +311,14 @@ class ndarray:
         from . import _reductions
         return _reductions.mean(self, axis, dtype, out, keepdims, where)
 
+    def cumsum(self, axis=None, dtype=None, out=None):
+        from . import _reductions
+        return _reductions.cumsum(self, axis, dtype, out)
+
+    def cumprod(self, axis=None, dtype=None, out=None):
+        from . import _reductions
+        return _reductions.cumprod(self, axis, dtype, out)
+
     def argmax(self, axis=None, out=None, keepdims=False):
         from . import _ufunc
         return _ufunc.argmax(self, axis, out, keepdims)

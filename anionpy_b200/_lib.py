@@ -75,6 +75,7 @@ _SIGS = {
     "ionp_accumulate": [ctypes.c_int32, _P, ctypes.c_int32, _P, ctypes.c_void_p],
     "ionp_reduceat": [ctypes.c_int32, _P, ctypes.c_int32, ctypes.POINTER(ctypes.c_int64), ctypes.c_int64, _P,
                       ctypes.c_void_p],
+    "ionp_at": [ctypes.c_int32, _P, ctypes.POINTER(ctypes.c_int64), ctypes.c_int64, _P, ctypes.c_void_p],
     "ionp_argext": [ctypes.c_int32, _P, ctypes.c_int32, ctypes.c_int32, _P, ctypes.c_void_p],
     "ionp_alloc": [ctypes.POINTER(ctypes.c_void_p), ctypes.c_size_t, ctypes.c_void_p],
     "ionp_free": [ctypes.c_void_p, ctypes.c_void_p],

@@ -20,6 +20,7 @@ as there, from an add reduction, dtype casts and a true divide:
 """
 from __future__ import annotations
 
+import builtins
 import ctypes
 import operator
 import warnings
@@ -31,7 +32,7 @@ from ._array import asarray, ndarray
 from ._lib import check, lib
 from ._ufunc import _NOVALUE, _normalize_axes, _scalar_result, add, logical_and, logical_or, maximum, minimum
 
-__all__ = ["sum", "prod", "min", "max", "amin", "amax", "any", "all", "mean"]
+__all__ = ["sum", "prod", "min", "max", "amin", "amax", "any", "all", "mean", "cumsum", "cumprod"]
 
 
 def _keepdims(k):
@@ -184,6 +185,46 @@ def mean(a, axis=None, dtype=None, out=None, keepdims=None, where=None):
     if final.ndim == 0:
         return _scalar_result(final)
     return final
+
+
+def _accumulate_axis(uf, a, axis, dtype, out):
+    """do_accumulate_axis (ionp-py/src/reductions.rs:1382): dtype= casts the
+    input first and the result last; axis=None (and any axis of a 0-d
+    array) accumulates the C-order ravel."""
+    arr = a if isinstance(a, ndarray) else asarray(a)
+    over = None if dtype is None else np.dtype(dtype)
+    if over is not None:
+        arr = arr._cast_to(over)
+    if axis is None:
+        target, ax = arr.reshape(-1), 0
+    else:
+        if isinstance(axis, (bool, np.bool_)) or isinstance(axis, float):
+            raise TypeError(f"'{type(axis).__name__}' object cannot be interpreted as an integer")
+        raw = operator.index(axis)
+        nd = arr.ndim
+        eff = builtins.max(nd, 1)  # this module's own max is the reduction
+        norm = raw + eff if raw < 0 else raw
+        if norm < 0 or norm >= eff:
+            from ._lib import AxisError
+            raise AxisError(f"axis {raw} is out of bounds for array of dimension {eff}")
+        target, ax = (arr.reshape(-1), 0) if nd == 0 else (arr, norm)
+    res = uf.accumulate(target, axis=ax)
+    if over is not None and res.dtype != over:
+        res = res._cast_to(over)
+    if out is not None:
+        return uf._write_out(res, out)
+    return res
+
+
+def cumsum(a, axis=None, dtype=None, out=None):
+    """add.accumulate along `axis` (default: the C-order ravel)."""
+    return _accumulate_axis(add, a, axis, dtype, out)
+
+
+def cumprod(a, axis=None, dtype=None, out=None):
+    """multiply.accumulate along `axis` (default: the C-order ravel)."""
+    from ._ufunc import multiply
+    return _accumulate_axis(multiply, a, axis, dtype, out)
 
 
 def _broadcast_to(m, shape):

@@ -298,6 +298,147 @@ class ufunc:
         return res
 
 
+    # ---- accumulate / reduceat / outer ------------------------------------
+    def _method_axis(self, a, axis, name):
+        """normalize_ufunc_method_axis (ionp-py/src/lib.rs:121)."""
+        nd = a.ndim
+        eff = max(nd, 1)
+        axis = operator.index(axis)
+        norm = axis + eff if axis < 0 else axis
+        if norm < 0 or norm >= eff:
+            raise AxisError(f"axis {axis} is out of bounds for array of dimension {nd}")
+        if nd == 0:
+            raise TypeError(f"cannot {name} on a scalar")
+        return norm
+
+    def _write_out(self, res, out):
+        """write_into_out_ufunc with casting='same_kind'."""
+        if isinstance(out, tuple):
+            out = out[0]
+        if not isinstance(out, ndarray):
+            raise TypeError("return arrays must be of ArrayType")
+        if out.shape != res.shape:
+            raise ValueError(f"non-broadcastable output operand with shape {out.shape} doesn't match the broadcast shape {res.shape}")
+        if not _can_cast(res.dtype, out.dtype, CAST_RULES["same_kind"]):
+            raise UFuncTypeError(f"Cannot cast ufunc '{self.__name__}' output from {res.dtype!r} to {out.dtype!r} with casting rule 'same_kind'")
+        if res.size:
+            check(lib().ionp_cast(ctypes.byref(res._desc()), ctypes.byref(out._desc()), None))
+        return out
+
+    def accumulate(self, array, axis=0, dtype=None, out=None):
+        """accumulate_axis (ionp-core/src/ufunc.rs:7967): every fiber along
+        `axis` folded in order; the result has the input's shape, its
+        order='K' layout and the reduce-family compute dtype. `dtype=` is
+        accepted and, like the reference, ignored."""
+        if self.nin != 2:
+            raise ValueError("accumulate only supported for binary functions")
+        a = array if isinstance(array, ndarray) else asarray(array)
+        ax = self._method_axis(a, axis, "accumulate")
+        L = lib()
+        r = ctypes.c_int32()
+        check(L.ionp_reduce_compute_dtype(self._op, code_of(a.dtype), ctypes.byref(r)))
+        cd = _dt(r.value)
+        descs = (ctypes.POINTER(IonpArr) * 1)(ctypes.pointer(a._desc()))
+        nd = a.ndim
+        sh = (ctypes.c_int64 * max(nd, 1))(*a.shape)
+        st = (ctypes.c_int64 * max(nd, 1))()
+        check(L.ionp_order_k_strides(1, descs, nd, sh, st))
+        res = ndarray.empty(a.shape, cd, list(st)[:nd])
+        if res.size:
+            check(L.ionp_accumulate(self._op, ctypes.byref(a._desc()), ax, ctypes.byref(res._desc()), None))
+        if out is not None:
+            return self._write_out(res, out)
+        return res
+
+    def reduceat(self, array, indices, axis=0, dtype=None, out=None):
+        """reduceat_binary_axis (ionp-core/src/ufunc.rs:8450): segment k of
+        every fiber along `axis` runs from indices[k] to indices[k+1] (the
+        axis end for the last) and is folded in order, or is the single
+        element indices[k] when the next index is not larger. C-ordered
+        result in the reduce-family compute dtype; `dtype=` is ignored, as
+        in the reference."""
+        if self.nin != 2:
+            raise ValueError("reduceat only supported for binary functions")
+        a = array if isinstance(array, ndarray) else asarray(array)
+        ax = self._method_axis(a, axis, "reduceat")
+        idx = np.asarray(indices)
+        if idx.dtype.kind not in "iu" and idx.size:
+            raise TypeError("Cannot cast array data from dtype('float64') to dtype('int64') according to the rule 'safe'")
+        idx = np.ascontiguousarray(idx.reshape(-1).astype(np.int64))
+        L = lib()
+        r = ctypes.c_int32()
+        check(L.ionp_reduce_compute_dtype(self._op, code_of(a.dtype), ctypes.byref(r)))
+        cd = _dt(r.value)
+        shape = list(a.shape)
+        shape[ax] = idx.size
+        res = ndarray.empty(tuple(shape), cd)
+        check(L.ionp_reduceat(self._op, ctypes.byref(a._desc()), ax,
+                              idx.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)), idx.size,
+                              ctypes.byref(res._desc()), None))
+        if out is not None:
+            return self._write_out(res, out)
+        return res
+
+    def outer(self, A, B):
+        """outer_binary (ionp-core/src/ufunc.rs:8212): op(A[i...], B[j...])
+        over the full cross product, shape A.shape + B.shape, C order: the
+        binary kernels on A viewed as A.shape + (1,) * B.ndim against B. Like
+        the reference (ionp-py/src/lib.rs:10091), no FPE report."""
+        if self.nin != 2:
+            raise ValueError("outer product only supported for binary functions")
+        a = A if isinstance(A, ndarray) else asarray(A)
+        b = B if isinstance(B, ndarray) else asarray(B)
+        av = ndarray(a._buf, tuple(a.shape) + (1,) * b.ndim, a.dtype, list(a.elem_strides) + [0] * b.ndim, a._off)
+        shape = tuple(a.shape) + tuple(b.shape)
+        rd = self._result_dtype([a.dtype, b.dtype])
+        res = ndarray.empty(shape, rd)
+        if res.size:
+            check(lib().ionp_binary(self._op, ctypes.byref(av._desc()), ctypes.byref(b._desc()), ctypes.byref(res._desc()),
+                                    None, None, None))
+        return res
+
+
+    def at(self, array, indices, b=None):
+        """ufunc.at (ionp-py/src/lib.rs:10160): in place on `array`,
+        array[indices[i], ...] = op(array[indices[i], ...], b[i, ...]) for i
+        in order (repeated indices apply again), b broadcast against
+        (len(indices),) + array.shape[1:]; unary ufuncs apply op once per
+        occurrence. Computed in the array's dtype (promoting ufuncs: on a
+        whole-array copy in the promoted dtype, cast back); no FPE report."""
+        if not isinstance(array, ndarray):
+            raise TypeError("first operand must be array")
+        idx = _at_indices(indices)
+        if self.nin == 1:
+            if b is not None:
+                raise TypeError("unary ufunc .at() takes no third argument")
+            values = None
+        else:
+            if b is None:
+                raise TypeError("binary ufunc .at() requires a values argument")
+            values = b if isinstance(b, ndarray) else asarray(b)
+        iv = np.ascontiguousarray(np.asarray(idx, dtype=np.int64).reshape(-1))
+        check(lib().ionp_at(self._op, ctypes.byref(array._desc()), iv.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)),
+                            iv.size, None if values is None else ctypes.byref(values._desc()), None))
+        return None
+
+
+def _at_indices(obj):
+    """extract_index_vec (ionp-py/src/lib.rs:8374): an int, or a sequence
+    of ints (an integer array included)."""
+    if isinstance(obj, ndarray):
+        obj = obj.get()
+    try:
+        return [operator.index(obj)]
+    except TypeError:
+        pass
+    if not isinstance(obj, (str, bytes)):
+        try:
+            return [operator.index(x) for x in obj]
+        except TypeError:
+            pass
+    raise TypeError("indices must be an int, a sequence of ints, or an integer numpy array")
+
+
 def _normalize_axes(axis, ndim):
     """normalize_reduce_axes (ionp-core/src/ufunc.rs:7551-7632)."""
     if axis is None:

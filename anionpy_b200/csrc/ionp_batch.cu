@@ -480,7 +480,7 @@ struct IonpBatch {
     std::vector<Orig> orig;
     std::vector<IonpSchedule> sched;
     int device = 0;
-    int sms = 148;
+    int sms = sm_count();
     // device state (from the caching allocator)
     BatchCall* d_calls = nullptr;
     int32_t* d_tile_call = nullptr;

@@ -317,9 +317,14 @@ int32_t check_arr(const IonpArr* a, const char* what) {
     if (!a) return set_err(IONP_ERR_INVALID, std::string(what) + " is NULL");
     if (a->ndim < 0 || a->ndim > IONP_MAX_DIMS) return set_err(IONP_ERR_INVALID, std::string(what) + ": ndim out of range");
     if (!dt_valid(a->dtype)) return set_err(IONP_ERR_UNSUPPORTED, std::string(what) + ": dtype not supported by this engine (complex/string)");
-    for (int i = 0; i < a->ndim; ++i)
+    int64_t total = 1;
+    for (int i = 0; i < a->ndim; ++i) {
         if (a->shape[i] < 0) return set_err(IONP_ERR_INVALID, std::string(what) + ": negative extent");
-    if (numel(a) > 0 && a->data == nullptr) return set_err(IONP_ERR_INVALID, std::string(what) + ": NULL data");
+        if (a->shape[i] > 0 && total > ((int64_t)1 << 62) / a->shape[i])
+            return set_err(IONP_ERR_INVALID, std::string(what) + ": more than 2^62 elements");
+        total *= a->shape[i];
+    }
+    if (total > 0 && a->data == nullptr) return set_err(IONP_ERR_INVALID, std::string(what) + ": NULL data");
     return IONP_OK;
 }
 
@@ -360,74 +365,126 @@ struct Block {
     cudaStream_t stream;
     cudaEvent_t ev;  // recorded at free time on `stream`
 };
-struct Allocator {
+// Caching device allocator: one pool per device (its own lock, free list
+// and counters). A freed block is cached with an event recorded on the
+// freeing stream; a later allocation from another stream waits for that
+// event before reuse. On a failed cudaMalloc the device's cached blocks
+// are released and the allocation retried once.
+struct DevicePool {
     std::mutex mu;
     std::multimap<size_t, Block> free_;   // by size
-    std::map<void*, Block> used_;
     uint64_t in_use = 0, cached = 0, peak = 0, mallocs = 0;
+};
+struct Allocator {
+    static constexpr int MAXDEV = 64;
+    DevicePool pools[MAXDEV];
+    std::mutex used_mu;
+    std::map<void*, std::pair<int, Block>> used_;   // pointer -> (device, block)
 
     static size_t round(size_t b) {
         if (b == 0) b = 1;
         if (b <= (1u << 20)) return (b + 511) & ~(size_t)511;
         return (b + (2u << 20) - 1) & ~(size_t)((2u << 20) - 1);
     }
+    static int32_t current_device(int* dev) {
+        if (cudaGetDevice(dev) != cudaSuccess) return cuda_err(cudaGetLastError(), "cudaGetDevice");
+        if (*dev < 0 || *dev >= MAXDEV) return set_err(IONP_ERR_INVALID, "device ordinal out of the allocator's range");
+        return IONP_OK;
+    }
     int32_t alloc(void** out, size_t bytes, cudaStream_t s) {
-        size_t sz = round(bytes);
-        std::lock_guard<std::mutex> g(mu);
-        auto it = free_.lower_bound(sz);
-        while (it != free_.end() && it->first <= sz + sz / 8) {
-            Block b = it->second;
-            if (b.stream != s && b.ev) cudaStreamWaitEvent(s, b.ev, 0);
-            free_.erase(it);
-            cached -= b.size;
-            b.stream = s;
-            used_[b.p] = b;
-            in_use += b.size;
-            peak = std::max(peak, in_use);
-            *out = b.p;
-            return IONP_OK;
-        }
-        void* p = nullptr;
-        cudaError_t e = cudaMalloc(&p, sz);
-        if (e != cudaSuccess) {
-            cudaGetLastError();
-            trim_locked();
-            e = cudaMalloc(&p, sz);
-            if (e != cudaSuccess) {
-                cudaGetLastError();
-                return set_err(IONP_ERR_OOM, "device allocation of " + std::to_string(sz) + " bytes failed: " + cudaGetErrorString(e));
+        int dev;
+        int32_t st = current_device(&dev);
+        if (st) return st;
+        const size_t sz = round(bytes);
+        DevicePool& P = pools[dev];
+        Block got{nullptr, 0, s, nullptr};
+        {
+            std::lock_guard<std::mutex> g(P.mu);
+            auto it = P.free_.lower_bound(sz);
+            if (it != P.free_.end() && it->first <= sz + sz / 8) {
+                got = it->second;
+                if (got.stream != s && got.ev) cudaStreamWaitEvent(s, got.ev, 0);
+                P.free_.erase(it);
+                P.cached -= got.size;
+                got.stream = s;
+                P.in_use += got.size;
+                P.peak = std::max(P.peak, P.in_use);
             }
         }
-        mallocs++;
-        Block b{p, sz, s, nullptr};
-        used_[p] = b;
-        in_use += sz;
-        peak = std::max(peak, in_use);
-        *out = p;
+        if (!got.p) {
+            void* p = nullptr;
+            cudaError_t e = cudaMalloc(&p, sz);
+            if (e != cudaSuccess) {
+                cudaGetLastError();
+                trim_device(dev);
+                e = cudaMalloc(&p, sz);
+                if (e != cudaSuccess) {
+                    cudaGetLastError();
+                    return set_err(IONP_ERR_OOM, "device allocation of " + std::to_string(sz) + " bytes failed: " + cudaGetErrorString(e));
+                }
+            }
+            got = Block{p, sz, s, nullptr};
+            std::lock_guard<std::mutex> g(P.mu);
+            P.mallocs++;
+            P.in_use += sz;
+            P.peak = std::max(P.peak, P.in_use);
+        }
+        {
+            std::lock_guard<std::mutex> g(used_mu);
+            used_[got.p] = {dev, got};
+        }
+        *out = got.p;
         return IONP_OK;
     }
     int32_t release(void* p, cudaStream_t s) {
         if (!p) return IONP_OK;
-        std::lock_guard<std::mutex> g(mu);
-        auto it = used_.find(p);
-        if (it == used_.end()) return set_err(IONP_ERR_INVALID, "ionp_free: pointer not from ionp_alloc");
-        Block b = it->second;
-        used_.erase(it);
-        in_use -= b.size;
+        int dev;
+        Block b;
+        {
+            std::lock_guard<std::mutex> g(used_mu);
+            auto it = used_.find(p);
+            if (it == used_.end()) return set_err(IONP_ERR_INVALID, "ionp_free: pointer not from ionp_alloc");
+            dev = it->second.first;
+            b = it->second.second;
+            used_.erase(it);
+        }
+        int cur = dev;
+        cudaGetDevice(&cur);
+        if (cur != dev) cudaSetDevice(dev);   // the event lives on the block's device
         if (!b.ev) cudaEventCreateWithFlags(&b.ev, cudaEventDisableTiming);
         b.stream = s;
         cudaEventRecord(b.ev, s);
-        free_.insert({b.size, b});
-        cached += b.size;
+        if (cur != dev) cudaSetDevice(cur);
+        DevicePool& P = pools[dev];
+        std::lock_guard<std::mutex> g(P.mu);
+        P.in_use -= b.size;
+        P.free_.insert({b.size, b});
+        P.cached += b.size;
         return IONP_OK;
     }
-    void trim_locked() {
-        for (auto& kv : free_) {
+    void trim_device(int dev) {
+        DevicePool& P = pools[dev];
+        std::lock_guard<std::mutex> g(P.mu);
+        int cur = dev;
+        cudaGetDevice(&cur);
+        if (cur != dev) cudaSetDevice(dev);
+        for (auto& kv : P.free_) {
             if (kv.second.ev) { cudaEventSynchronize(kv.second.ev); cudaEventDestroy(kv.second.ev); }
             cudaFree(kv.second.p);
         }
-        free_.clear();
-        cached = 0;
+        if (cur != dev) cudaSetDevice(cur);
+        P.free_.clear();
+        P.cached = 0;
+    }
+    void trim_all() {
+        for (int d = 0; d < MAXDEV; ++d) {
+            bool any;
+            {
+                std::lock_guard<std::mutex> g(pools[d].mu);
+                any = !pools[d].free_.empty();
+            }
+            if (any) trim_device(d);
+        }
     }
 };
 Allocator& allocator() {
@@ -439,12 +496,59 @@ std::atomic<uint64_t> g_launches{0};
 
 void count_launch(int k) { g_launches.fetch_add((uint64_t)k, std::memory_order_relaxed); }
 
+int sm_count() {
+    static std::atomic<int> cache[64];
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) { cudaGetLastError(); return 148; }
+    int v = cache[dev].load(std::memory_order_relaxed);
+    if (v > 0) return v;
+    int n = 0;
+    if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n <= 0) {
+        cudaGetLastError();
+        n = 148;  // a B200's count, for planning only
+    }
+    cache[dev].store(n, std::memory_order_relaxed);
+    return n;
+}
+
 void* scratch_alloc(size_t bytes, cudaStream_t s) {
     void* p = nullptr;
     if (allocator().alloc(&p, bytes, s) != IONP_OK) return nullptr;
     return p;
 }
 void scratch_free(void* p, cudaStream_t s) { allocator().release(p, s); }
+
+static std::mutex g_err_mu;
+static uint32_t* g_err_word[256] = {nullptr};
+
+uint32_t* async_error_word() {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 256) return nullptr;
+    std::lock_guard<std::mutex> g(g_err_mu);
+    if (!g_err_word[dev]) {
+        void* p = nullptr;
+        if (cudaMalloc(&p, 256) != cudaSuccess) { cudaGetLastError(); return nullptr; }
+        if (cudaMemset(p, 0, 256) != cudaSuccess) { cudaFree(p); cudaGetLastError(); return nullptr; }
+        g_err_word[dev] = (uint32_t*)p;
+    }
+    return g_err_word[dev];
+}
+
+int32_t check_async_error() {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 256) return IONP_OK;
+    uint32_t* w;
+    {
+        std::lock_guard<std::mutex> g(g_err_mu);
+        w = g_err_word[dev];
+    }
+    if (!w) return IONP_OK;
+    uint32_t v = 0;
+    if (cudaMemcpy(&v, w, sizeof(v), cudaMemcpyDeviceToHost) != cudaSuccess) return cuda_err(cudaGetLastError(), "error word read");
+    if (!v) return IONP_OK;
+    cudaMemset(w, 0, sizeof(uint32_t));
+    return set_err(IONP_ERR_TIMEOUT, "a kernel's bounded wait for a bulk copy gave up; its results are incomplete");
+}
 
 static thread_local uint32_t* t_pinned_flag = nullptr;
 
@@ -696,16 +800,17 @@ int32_t ionp_alloc(void** ptr, size_t bytes, IonpStream stream) {
 }
 int32_t ionp_free(void* ptr, IonpStream stream) { return allocator().release(ptr, (cudaStream_t)stream); }
 int32_t ionp_alloc_stats(uint64_t* s) {
-    if (!s) return IONP_ERR_INVALID;
-    Allocator& A = allocator();
-    std::lock_guard<std::mutex> g(A.mu);
-    s[0] = A.in_use; s[1] = A.cached; s[2] = A.peak; s[3] = A.mallocs;
+    if (!s) return set_err(IONP_ERR_INVALID, "ionp_alloc_stats: NULL stats pointer");
+    int dev;
+    int32_t st = Allocator::current_device(&dev);
+    if (st) return st;
+    DevicePool& P = allocator().pools[dev];
+    std::lock_guard<std::mutex> g(P.mu);
+    s[0] = P.in_use; s[1] = P.cached; s[2] = P.peak; s[3] = P.mallocs;
     return IONP_OK;
 }
 int32_t ionp_alloc_trim(void) {
-    Allocator& A = allocator();
-    std::lock_guard<std::mutex> g(A.mu);
-    A.trim_locked();
+    allocator().trim_all();
     return IONP_OK;
 }
 
@@ -1075,8 +1180,14 @@ int32_t ionp_stream_create(IonpStream* stream) {
     return st;
 }
 int32_t ionp_stream_destroy(IonpStream stream) { return cuda_err(cudaStreamDestroy((cudaStream_t)stream), "stream destroy"); }
-int32_t ionp_stream_synchronize(IonpStream stream) { return cuda_err(cudaStreamSynchronize((cudaStream_t)stream), "stream synchronize"); }
-int32_t ionp_device_synchronize(void) { return cuda_err(cudaDeviceSynchronize(), "device synchronize"); }
+int32_t ionp_stream_synchronize(IonpStream stream) {
+    int32_t st = cuda_err(cudaStreamSynchronize((cudaStream_t)stream), "stream synchronize");
+    return st ? st : check_async_error();
+}
+int32_t ionp_device_synchronize(void) {
+    int32_t st = cuda_err(cudaDeviceSynchronize(), "device synchronize");
+    return st ? st : check_async_error();
+}
 int32_t ionp_host_alloc(void** ptr, size_t bytes) { return cuda_err(cudaMallocHost(ptr, bytes ? bytes : 1), "pinned alloc"); }
 int32_t ionp_host_free(void* ptr) { return cuda_err(cudaFreeHost(ptr), "pinned free"); }
 int32_t ionp_event_create(void** ev) {
@@ -1098,8 +1209,10 @@ int32_t ionp_device_info(int32_t* count, int32_t* sm_count, char* name, size_t l
     if (cudaGetDeviceCount(&n) != cudaSuccess) { cudaGetLastError(); n = 0; }
     if (count) *count = n;
     if (n == 0) return IONP_OK;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) { cudaGetLastError(); dev = 0; }
     cudaDeviceProp p;
-    int32_t st = cuda_err(cudaGetDeviceProperties(&p, 0), "device properties");
+    int32_t st = cuda_err(cudaGetDeviceProperties(&p, dev), "device properties");
     if (st) return st;
     if (sm_count) *sm_count = p.multiProcessorCount;
     if (name && len) { strncpy(name, p.name, len - 1); name[len - 1] = 0; }

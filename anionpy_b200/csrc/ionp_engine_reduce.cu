@@ -99,12 +99,28 @@ int32_t run_row(RedDesc& d, cudaStream_t s) {
     }
     // more parallel units when there are few outputs and long runs: the
     // wide-row kernels take a warp (float add) or a CTA per unit
-    int64_t want = 148 * 2;
+    int64_t want = sm_count() * 2;
     if (row_wide_ok(d, dt_bytes(d.cd))) {
-        if (rowst_type_ok(d.op, d.cd)) want = 148 * 16;
-        else if (rowco_type_ok(d.op, d.cd)) want = 148 * RCO_CTAS;
+        if (rowst_type_ok(d.op, d.cd)) want = sm_count() * 16;
+        else if (rowco_type_ok(d.op, d.cd)) want = sm_count() * RCO_CTAS;
     }
     while ((d.nout << K) < want && *seg_lengths(w, K + 1).begin() >= 4096 && K < 20 && K < 2 * TOP_CHUNK_LOG) ++K;
+    // float32 add over a power-of-two run: one 4096-element window per unit
+    // (the window kernel then balances evenly over all warps, and the top
+    // pass folds the window sums as the perfect tree they form)
+    {
+        RedDesc t = d;
+        t.K = 0;
+        if (pw32_ok(t)) {
+            // units of 2^p windows, p as large as keeps >= 8 units per warp
+            int kw = 0;
+            while ((w >> kw) > PW32_WIN) ++kw;
+            const int64_t want_units = (int64_t)sm_count() * 6 * 8;
+            int kk = kw;
+            while (kk > 0 && (d.nout << (kk - 1)) >= want_units) --kk;
+            if (kk <= 2 * TOP_CHUNK_LOG && kk >= K) K = kk;
+        }
+    }
     auto lens = seg_lengths(w, K);
     int64_t maxlen = *lens.rbegin();
     std::map<int64_t, int> memo;
@@ -119,7 +135,7 @@ int32_t run_row(RedDesc& d, cudaStream_t s) {
     d.D = D;
     const int64_t ntasks = d.nout << K;
     int64_t g = (ntasks + groups - 1) / groups;
-    int64_t cap = 148LL * (tpr == 256 ? 8 : 8);
+    int64_t cap = (int64_t)sm_count() * (tpr == 256 ? 8 : 8);
     int grid = (int)std::max<int64_t>(1, std::min(g, cap));
     void* scratch = nullptr;
     if (K > 0) {
@@ -127,6 +143,7 @@ int32_t run_row(RedDesc& d, cudaStream_t s) {
         if (!scratch) return IONP_ERR_OOM;
         d.scratch = scratch;
     }
+    d.err = async_error_word();
     int32_t st = cuda_err(launch_reduce_row(d, tpr, smem, grid, s), "reduce row launch");
     if (!st && K > 0) st = cuda_err(launch_reduce_row_top(d, s), "reduce top launch");
     if (scratch) scratch_free(scratch, s);
@@ -396,7 +413,7 @@ int32_t ionp_reduce(int32_t op, const IonpArr* a_in, const int32_t* axes, int32_
         // too few outputs for one thread each to keep HBM busy: cut the
         // axis into 2^K parts and fold the parts in order on top
         int K = 0;
-        while (d.nout < 65536 && (d.nout << K) < 148 * 2048 && (d.rshape[0] >> (K + 1)) >= 256 && K < 10) ++K;
+        while (d.nout < 65536 && (d.nout << K) < sm_count() * 2048 && (d.rshape[0] >> (K + 1)) >= 256 && K < 10) ++K;
         if (K > 0) {
             d.K = K;
             void* scratch = scratch_alloc((size_t)(d.nout << K) * dt_bytes(cd), s);
@@ -462,15 +479,15 @@ int32_t ionp_argext(int32_t is_max, const IonpArr* a, int32_t axis, int32_t keep
         d.rst[0] = d.ws = a->strides[axis];
         int64_t min_kept = INT64_MAX;
         for (int i = 0; i < nd; ++i) if (i != axis && a->shape[i] > 1) min_kept = std::min<int64_t>(min_kept, std::llabs(a->strides[i]));
-        if (std::llabs(d.ws) > min_kept && d.nout >= 148 * 32) mode = 1;  // column scan
+        if (std::llabs(d.ws) > min_kept && d.nout >= sm_count() * 32) mode = 1;  // column scan
     }
-    if (mode == 0 && axis != -1 && d.nr == 1 && d.ws == 1 && d.nk == 1 && d.kst[0] == d.w && d.nout >= 148 * 256 &&
+    if (mode == 0 && axis != -1 && d.nr == 1 && d.ws == 1 && d.nk == 1 && d.kst[0] == d.w && d.nout >= sm_count() * 256 &&
         (d.w * dt_bytes(d.cd)) % 16 == 0 && d.w * dt_bytes(d.cd) <= 256 && reinterpret_cast<uintptr_t>(d.a) % 16 == 0)
         return cuda_err(launch_argext(d, is_max, 3, tpr, s), "argext narrow launch");
     if (mode == 0) {
         tpr = d.w < 64 ? 1 : d.w <= 4096 ? 32 : 256;
         int K = 0;
-        while ((d.nout << K) < 148 * 4 && (d.w >> (K + 1)) >= 8192 && K < 16) ++K;
+        while ((d.nout << K) < sm_count() * 4 && (d.w >> (K + 1)) >= 8192 && K < 16) ++K;
         d.K = K;
         void* scratch = nullptr;
         if (K > 0) {
@@ -486,7 +503,7 @@ int32_t ionp_argext(int32_t is_max, const IonpArr* a, int32_t axis, int32_t keep
     }
     // column scan; split the axis when the outputs alone leave HBM idle
     int K = 0;
-    while ((d.nout << K) < 148 * 2048 && (d.w >> (K + 1)) >= 256 && K < 10) ++K;
+    while ((d.nout << K) < sm_count() * 2048 && (d.w >> (K + 1)) >= 256 && K < 10) ++K;
     d.K = K;
     void* scratch = nullptr;
     if (K > 0) {

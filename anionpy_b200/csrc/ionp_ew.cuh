@@ -471,7 +471,7 @@ k_un_nd(EwDesc d, uint32_t* flags) {
 // 148 SMs at full occupancy, fewer for small problems.
 inline int ew_grid(int64_t work_items) {
     int64_t want = (work_items + EW_THREADS - 1) / EW_THREADS;
-    int64_t cap = 148LL * 8;  // 8 resident 256-thread CTAs per SM
+    int64_t cap = (int64_t)sm_count() * 8;  // 8 resident 256-thread CTAs per SM
     if (want < 1) want = 1;
     return (int)(want < cap ? want : cap);
 }

@@ -65,7 +65,7 @@ cudaError_t launch_bin_t(const EwDesc& d, const ContigInfo& ci, uint32_t* flags,
                 if (trv_ok<T>(d)) {
                     constexpr int TL = TrV<T>::TILE;
                     const int64_t tiles = (d.shape[0] / TL) * (d.shape[1] / TL);
-                    const int g = (int)(tiles < 148 * 6 ? tiles : 148 * 6);
+                    const int g = (int)(tiles < sm_count() * 6 ? tiles : sm_count() * 6);
                     if constexpr (HAS_FPE) {
                         if (fpe) { k_bin_trv<OP, CD, true><<<g, EW_THREADS, 0, s>>>(d, flags); count_launch(); return cudaGetLastError(); }
                     }
@@ -75,7 +75,7 @@ cudaError_t launch_bin_t(const EwDesc& d, const ContigInfo& ci, uint32_t* flags,
                 }
             }
             const int64_t tiles = ((d.shape[0] + TR_TILE - 1) / TR_TILE) * ((d.shape[1] + TR_TILE - 1) / TR_TILE);
-            const int g = (int)(tiles < 148 * 8 ? tiles : 148 * 8);
+            const int g = (int)(tiles < sm_count() * 8 ? tiles : sm_count() * 8);
             if constexpr (HAS_FPE) {
                 if (fpe) { k_bin_tr<OP, CD, true><<<g, EW_THREADS, 0, s>>>(d, flags); count_launch(); return cudaGetLastError(); }
             }

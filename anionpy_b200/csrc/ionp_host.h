@@ -64,6 +64,13 @@ void scratch_free(void* p, cudaStream_t s);
 
 // FPE word helpers: device flag word from the allocator, read back after the
 // stream drains.
+// One device word per device that kernels set when a bounded wait of theirs
+// gives up (a bulk copy that never completes); null if it cannot be had.
+// ionp_stream_synchronize / ionp_device_synchronize report it as
+// IONP_ERR_TIMEOUT and clear it.
+uint32_t* async_error_word();
+int32_t check_async_error();
+
 struct FlagWord {
     uint32_t* d = nullptr;
     cudaStream_t s = nullptr;

@@ -37,6 +37,8 @@ struct ContigInfo {
 // Launchers (defined in the kernel files). Return a cudaError_t.
 cudaError_t launch_binary(int op, int cd, const EwDesc& d, const ContigInfo& ci, uint32_t* dflags, cudaStream_t s);
 cudaError_t launch_unary(int op, int cd, const EwDesc& d, const ContigInfo& ci, uint32_t* dflags, cudaStream_t s);
+// streaming multiprocessors of the current device (queried once per device)
+int sm_count();
 cudaError_t launch_cast(const EwDesc& d, cudaStream_t s);
 cudaError_t launch_cast_check(const EwDesc& d, double lo, double hi, uint32_t* flags, cudaStream_t s);
 // FPE detector with the reference's flat `x[i % len]` operand pairing, for

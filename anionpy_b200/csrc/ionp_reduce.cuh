@@ -76,6 +76,9 @@ struct RedDesc {
     int32_t D;       // slot-tree depth of one segment
     int32_t Dw, Dl;  // wide-row staged kernel: window depth, leaf-slot depth
     void* scratch;
+    // a device word a kernel sets when one of its bounded waits gives up
+    // (null: none); the library reports it at the next synchronization
+    uint32_t* err;
     // masked
     const uint8_t* m;
     int64_t mkst[RD_MAXD], mrst[RD_MAXD], mwst_raw[RD_MAXD];
@@ -400,13 +403,13 @@ __global__ void __launch_bounds__(RED_THREADS, 4) k_red_row(RedDesc d) {
 // binary tree (adjacent pairs, left operand first), then seed and store.
 // The partials are folded in chunks of 2^KC (each chunk is a perfect
 // subtree of the same tree); the 2^(K - KC) chunk results then fold as the
-// tree's top levels, so shared memory stays at TOP_CHUNK + 2^(K - KC) values
-// for any K <= 2 TOP_CHUNK_LOG.
+// tree's top levels, so shared memory stays at 2^(K - KC) values plus one per
+// warp for any K <= 2 TOP_CHUNK_LOG.
 constexpr int TOP_CHUNK_LOG = 11;
 __host__ __device__ constexpr int top_chunk_log(int K) { return K < TOP_CHUNK_LOG ? K : TOP_CHUNK_LOG; }
 template <class A>
 __host__ __device__ constexpr size_t row_top_smem(int K) {
-    return (((size_t)1 << top_chunk_log(K)) + ((size_t)1 << (K - top_chunk_log(K)))) * sizeof(A);
+    return (((size_t)1 << (K - top_chunk_log(K))) + RED_THREADS / 32) * sizeof(A);
 }
 template <int OP, int CD>
 __global__ void __launch_bounds__(RED_THREADS) k_red_row_top(RedDesc d) {
@@ -415,26 +418,45 @@ __global__ void __launch_bounds__(RED_THREADS) k_red_row_top(RedDesc d) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int kc = top_chunk_log(d.K);
     const int csize = 1 << kc, nchunk = 1 << (d.K - kc);
-    A* v = reinterpret_cast<A*>(smem_raw);
-    A* top = v + csize;
+    A* top = reinterpret_cast<A*>(smem_raw);          // nchunk chunk totals
+    A* wsum = top + nchunk;                            // RED_THREADS / 32 warp totals
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int64_t nseg = (int64_t)1 << d.K;
     for (int64_t o = blockIdx.x; o < d.nout; o += gridDim.x) {
         for (int c = 0; c < nchunk; ++c) {
             const A* part = reinterpret_cast<const A*>(d.scratch) + o * nseg + (int64_t)c * csize;
-            for (int s = threadIdx.x; s < csize; s += blockDim.x) v[s] = part[s];
-            __syncthreads();
-            for (int half = 1; half < csize; half <<= 1) {
-                for (int s = threadIdx.x * 2 * half; s < csize; s += blockDim.x * 2 * half) v[s] = P::fold(v[s], v[s + half]);
-                __syncthreads();
+            // thread t folds partials [t m, (t + 1) m) in registers (m a power of
+            // two), warps fold 32 such blocks by shuffles, then the warp totals
+            // fold in one thread: each step joins adjacent perfect subtrees,
+            // left operand first, so the whole is the chunk's perfect tree
+            const int m = csize > RED_THREADS ? csize / RED_THREADS : 1;
+            const int active = csize > RED_THREADS ? RED_THREADS : csize;
+            A v{};
+            if ((int)threadIdx.x < active) {
+                A x[8];
+                for (int i = 0; i < m; ++i) x[i] = part[threadIdx.x * m + i];
+                for (int h = 1; h < m; h <<= 1)
+                    for (int i = 0; i < m; i += 2 * h) x[i] = P::fold(x[i], x[i + h]);
+                v = x[0];
             }
-            if (threadIdx.x == 0) top[c] = v[0];
+            const int wl = active < 32 ? active : 32;  // leaves of each warp's tree
+            for (int h = 1; h < wl; h <<= 1) {
+                const A ov = __shfl_down_sync(0xffffffffu, v, h);
+                if ((lane & (2 * h - 1)) == 0 && lane + h < wl) v = P::fold(v, ov);
+            }
+            if (lane == 0) wsum[warp] = v;
             __syncthreads();
-        }
-        for (int half = 1; half < nchunk; half <<= 1) {
-            for (int s = threadIdx.x * 2 * half; s < nchunk; s += blockDim.x * 2 * half) top[s] = P::fold(top[s], top[s + half]);
+            if (threadIdx.x == 0) {
+                const int nw = active / 32 > 1 ? active / 32 : 1;
+                for (int h = 1; h < nw; h <<= 1)
+                    for (int i = 0; i < nw; i += 2 * h) wsum[i] = P::fold(wsum[i], wsum[i + h]);
+                top[c] = wsum[0];
+            }
             __syncthreads();
         }
         if (threadIdx.x == 0) {
+            for (int h = 1; h < nchunk; h <<= 1)
+                for (int i = 0; i < nchunk; i += 2 * h) top[i] = P::fold(top[i], top[i + h]);
             int64_t in_off, out_off;
             kept_offsets(d, o, &in_off, &out_off);
             store_cast<CD>(d.o, out_off, d.odt, P::finish(top[0], d.has_seed, d.seed));

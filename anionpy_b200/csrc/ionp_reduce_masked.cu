@@ -7,7 +7,7 @@ template <int OPV>
 static cudaError_t masked_op(const RedDesc& d, cudaStream_t s) {
     int64_t g = (d.nout + 127) / 128;
     if (g < 1) g = 1;
-    if (g > 148 * 16) g = 148 * 16;
+    if (g > sm_count() * 16) g = sm_count() * 16;
 #define IONP_DTCASE(D)                                                     \
     case D:                                                                \
         if constexpr (red_any_valid(OPV, D)) {                             \

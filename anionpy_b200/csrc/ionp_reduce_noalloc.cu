@@ -233,7 +233,7 @@ extern "C" int32_t ionp_reduce_noalloc(int32_t op, const IonpArr* a, const int32
                                            std::to_string((size_t)(d.nout << K) * acc) + " bytes) exceed the " +
                                            std::to_string((size_t)IONP_NOALLOC_SCRATCH_BYTES) +
                                            "-byte static scratch; use ionp_reduce");
-    while ((d.nout << K) < 148 * 2 && *lengths_at(w, K + 1).begin() >= 4096 && K < 20 && fits(K + 1)) ++K;
+    while ((d.nout << K) < sm_count() * 2 && *lengths_at(w, K + 1).begin() >= 4096 && K < 20 && fits(K + 1)) ++K;
     auto lens = lengths_at(w, K);
     int D = 0;
     for (int64_t l : lens) D = std::max(D, tree_depth(l));
@@ -244,7 +244,7 @@ extern "C" int32_t ionp_reduce_noalloc(int32_t op, const IonpArr* a, const int32
     d.K = K;
     d.D = D;
     const int64_t ntasks = d.nout << K;
-    const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((ntasks + groups - 1) / groups, 148LL * 8));
+    const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((ntasks + groups - 1) / groups, (int64_t)sm_count() * 8));
     if (K > 0) {
         // Every partial the top pass reads is written by the row pass of the
         // same call, so the array needs no clearing between calls.

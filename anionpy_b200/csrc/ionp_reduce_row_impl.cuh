@@ -34,9 +34,9 @@ template <int OP, int CD>
 static cudaError_t row_top_t(const RedDesc& d, cudaStream_t s) {
     typedef typename RPol<OP, CD>::A A;
     if constexpr (red_assoc(OP, CD)) {
-        if (d.K <= 6 && d.nout >= 148 * 8) {
+        if (d.K <= 6 && d.nout >= sm_count() * 8) {
             int64_t g = (d.nout + RED_THREADS - 1) / RED_THREADS;
-            if (g > 148 * 16) g = 148 * 16;
+            if (g > sm_count() * 16) g = sm_count() * 16;
             k_red_row_top_small<OP, CD><<<(int)g, RED_THREADS, 0, s>>>(d);
             count_launch();
             return cudaGetLastError();
@@ -44,7 +44,7 @@ static cudaError_t row_top_t(const RedDesc& d, cudaStream_t s) {
     }
     if (d.K > 2 * TOP_CHUNK_LOG) return cudaErrorInvalidValue;   // planners cap K far below this
     const size_t smem = row_top_smem<A>(d.K);                    // at most 32 KiB
-    int grid = (int)(d.nout < 148 * 8 ? d.nout : 148 * 8);
+    int grid = (int)(d.nout < sm_count() * 8 ? d.nout : sm_count() * 8);
     k_red_row_top<OP, CD><<<grid, RED_THREADS, smem, s>>>(d);
     count_launch();
     return cudaGetLastError();

@@ -698,6 +698,204 @@ __global__ void __launch_bounds__(RED_THREADS, NAR_CTAS) k_red_rownar(RedDesc d)
 // ---------------------------------------------------------------------------
 // Host side: which rows take these kernels, and their launch.
 // ---------------------------------------------------------------------------
+// ---------------------------------------------------------------------------
+// k_red_pw32: float32 add over runs of 2^m >= 4096 elements, the common
+// case of a row or whole-array sum. For such runs numpy's pairwise tree
+// (ufunc.rs:6416-6448) halves exactly down to 128-element leaves, so the
+// run is a perfect tree of 4096-element windows, each a perfect tree of 32
+// leaves. One warp takes one window at a time:
+//  * load: every lane issues one 512-byte bulk copy (cp.async.bulk, the TMA
+//    engine, unicast from this GPU's memory) of its leaf into a padded
+//    shared slot, completing on the stage's mbarrier; two stages per warp;
+//  * leaf: the lane sums its 128 elements as 8 independent chains of plain
+//    adds (elements k, k+8, ...), combined ((r0+r1)+(r2+r3))+((r4+r5)+
+//    (r6+r7)). A chain that comes out NaN is summed again with the engine's
+//    add (the x86 NaN rules) and the combine redone with it: a result that
+//    is not NaN had no NaN in it, so plain adds give the same bits;
+//  * window: the 32 leaf sums fold across lanes by shuffles, left operand
+//    first (a perfect tree);
+//  * run: window sums fold on a binary-counter stack (push; while the two
+//    top entries have the same height, fold them), which rebuilds the
+//    perfect tree over a unit's 2^p windows.
+// Every mbarrier wait has an iteration limit; a wait that gives up sets
+// d.err, drains the warp's copies (again with a limit) and ends the warp.
+// ---------------------------------------------------------------------------
+constexpr int PW32_WIN = 4096;
+constexpr int PW32_PITCH = 132;      // floats per shared leaf slot (16 bytes of padding)
+constexpr int PW32_STAGES = 2;
+constexpr int PW32_WARPS = 2;
+constexpr int PW32_STACK = 24;
+constexpr size_t PW32_STAGE_BYTES = (size_t)32 * PW32_PITCH * sizeof(float);
+constexpr size_t PW32_WARP_SMEM = PW32_STAGES * PW32_STAGE_BYTES + 64 + PW32_STACK * 8;
+constexpr size_t PW32_SMEM = PW32_WARPS * PW32_WARP_SMEM;
+constexpr long long PW32_SPIN_LIMIT = 1LL << 26;
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, unsigned count) {
+    const unsigned a = (unsigned)__cvta_generic_to_shared(bar);
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(a), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, unsigned bytes) {
+    const unsigned a = (unsigned)__cvta_generic_to_shared(bar);
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(a), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, unsigned parity) {
+    const unsigned a = (unsigned)__cvta_generic_to_shared(bar);
+    unsigned ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok) : "r"(a), "r"(parity) : "memory");
+    return ok != 0;
+}
+// bounded wait for the phase with the given parity to complete
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, unsigned parity) {
+    for (long long i = 0; i < PW32_SPIN_LIMIT; ++i)
+        if (mbar_try_wait(bar, parity)) return true;
+    return false;
+}
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned bytes, uint64_t* bar) {
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    const unsigned b = (unsigned)__cvta_generic_to_shared(bar);
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n"
+                 ::"r"(d), "l"(src), "r"(bytes), "r"(b) : "memory");
+}
+
+template <int OP, int CD>
+__global__ void __launch_bounds__(32 * PW32_WARPS) k_red_pw32(RedDesc d) {
+    typedef RPol<OP, CD> P;
+    static_assert(CD == DT_F32 && OP == OP_ADD, "float32 add only");
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    unsigned char* wb = smem_raw + (size_t)warp * PW32_WARP_SMEM;
+    float* ring = reinterpret_cast<float*>(wb);
+    uint64_t* bar = reinterpret_cast<uint64_t*>(wb + PW32_STAGES * PW32_STAGE_BYTES);
+    float* stk = reinterpret_cast<float*>(bar + 8);
+    int* stk_h = reinterpret_cast<int*>(stk + PW32_STACK);
+    const int64_t nseg = (int64_t)1 << d.K;
+    const int64_t nunits = d.nout * nseg;
+    const int64_t seglen = d.w >> d.K;
+    const int64_t wpu = seglen / PW32_WIN;
+    const int64_t gw = (int64_t)blockIdx.x * PW32_WARPS + warp, GW = (int64_t)gridDim.x * PW32_WARPS;
+    const int64_t myunits = nunits > gw ? (nunits - gw + GW - 1) / GW : 0;
+    const float* a = reinterpret_cast<const float*>(d.a);
+    if (lane == 0) {
+        for (int s = 0; s < PW32_STAGES; ++s) mbar_init(&bar[s], 1);
+        asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+        asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+    }
+    __syncwarp();
+    auto unit_base = [&](int64_t ui) -> const float* {
+        const int64_t u = gw + ui * GW;
+        int64_t in_off, out_off;
+        kept_offsets(d, u >> d.K, &in_off, &out_off);
+        return a + in_off + (u & (nseg - 1)) * seglen;
+    };
+    // the issue cursor runs PW32_STAGES - 1 windows ahead of the fold
+    int64_t iu = 0, ij = 0, iq = 0;
+    const float* ibase = myunits > 0 ? unit_base(0) : a;
+    auto issue = [&]() {
+        if (iu >= myunits) return;
+        const int s = (int)(iq % PW32_STAGES);
+        if (lane == 0) mbar_expect_tx(&bar[s], 32 * 512);
+        __syncwarp();
+        bulk_g2s(ring + (size_t)s * 32 * PW32_PITCH + lane * PW32_PITCH, ibase + ij * PW32_WIN + lane * 128, 512, &bar[s]);
+        ++iq;
+        if (++ij == wpu) {
+            ij = 0;
+            if (++iu < myunits) ibase = unit_base(iu);
+        }
+    };
+    for (int s = 0; s < PW32_STAGES - 1; ++s) issue();
+    int top = 0;  // stack entries (lane 0)
+    int64_t q = 0;
+    for (int64_t ui = 0; ui < myunits; ++ui) {
+        for (int64_t j = 0; j < wpu; ++j, ++q) {
+            issue();
+            const int s = (int)(q % PW32_STAGES);
+            if (!mbar_wait_bounded(&bar[s], (unsigned)((q / PW32_STAGES) & 1))) {
+                // give up: record it, drain this warp's other copy, end the warp
+                if (lane == 0 && d.err) atomicOr(d.err, 1u);
+                if (iq > q + 1) mbar_wait_bounded(&bar[(q + 1) % PW32_STAGES], (unsigned)(((q + 1) / PW32_STAGES) & 1));
+                return;
+            }
+            const float* lp = ring + (size_t)s * 32 * PW32_PITCH + lane * PW32_PITCH;
+            float r[8];
+#pragma unroll
+            for (int jj = 0; jj < 16; ++jj) {
+                const float4 x0 = *reinterpret_cast<const float4*>(lp + 8 * jj);
+                const float4 x1 = *reinterpret_cast<const float4*>(lp + 8 * jj + 4);
+                const float x[8] = {x0.x, x0.y, x0.z, x0.w, x1.x, x1.y, x1.z, x1.w};
+#pragma unroll
+                for (int k = 0; k < 8; ++k) r[k] = jj == 0 ? x[k] : __fadd_rn(r[k], x[k]);
+            }
+            float leaf = __fadd_rn(__fadd_rn(__fadd_rn(r[0], r[1]), __fadd_rn(r[2], r[3])),
+                                   __fadd_rn(__fadd_rn(r[4], r[5]), __fadd_rn(r[6], r[7])));
+            if (leaf != leaf) {
+                // Only the first NaN chain needs the exact replay: in the
+                // left-first combine tree it is left of every later chain
+                // at their common node, so a later NaN never wins; earlier
+                // chains are NaN-free and exact, and an inf - inf among
+                // them is redone by the exact combine below.
+                int kf = 7;
+#pragma unroll
+                for (int k = 6; k >= 0; --k) kf = (r[k] != r[k]) ? k : kf;
+                float acc = lp[kf];
+#pragma unroll 1
+                for (int i = 1; i < 16; ++i) acc = P::fold(acc, lp[kf + 8 * i]);
+#pragma unroll
+                for (int k = 0; k < 8; ++k) r[k] = (k == kf) ? acc : r[k];
+                leaf = P::fold(P::fold(P::fold(r[0], r[1]), P::fold(r[2], r[3])),
+                               P::fold(P::fold(r[4], r[5]), P::fold(r[6], r[7])));
+            }
+            __syncwarp();  // every lane has read this stage before it is refilled
+            float v = leaf;
+#pragma unroll
+            for (int h = 1; h < 32; h <<= 1) {
+                const float o = __shfl_down_sync(0xffffffffu, v, h);
+                if ((lane & (2 * h - 1)) == 0) v = P::fold(v, o);
+            }
+            if (lane == 0) {
+                if (wpu == 1) {
+                    stk[0] = v;
+                } else {
+                    stk[top] = v;
+                    stk_h[top] = 0;
+                    ++top;
+                    while (top >= 2 && stk_h[top - 1] == stk_h[top - 2]) {
+                        stk[top - 2] = P::fold(stk[top - 2], stk[top - 1]);
+                        stk_h[top - 2] += 1;
+                        --top;
+                    }
+                }
+                if (j == wpu - 1) {
+                    const int64_t u = gw + ui * GW;
+                    const float total = stk[0];
+                    top = 0;
+                    if (d.K == 0) {
+                        int64_t in_off, out_off;
+                        kept_offsets(d, u, &in_off, &out_off);
+                        store_cast<CD>(d.o, out_off, d.odt, P::finish(total, d.has_seed, d.seed));
+                    } else {
+                        reinterpret_cast<float*>(d.scratch)[u] = total;
+                    }
+                }
+            }
+        }
+    }
+}
+
+// Runs k_red_pw32 handles: float32 add, input contiguous along the run in
+// float32, 16-byte aligned run starts, a power-of-two run of at least one
+// window whose K-level segments are whole windows.
+inline bool pw32_ok(const RedDesc& d) {
+    if (d.op != OP_ADD || d.cd != DT_F32 || d.adt != DT_F32 || d.ws != 1) return false;
+    if (d.w < PW32_WIN || (d.w & (d.w - 1)) != 0) return false;
+    if ((d.w >> d.K) < PW32_WIN) return false;
+    if ((reinterpret_cast<uintptr_t>(d.a) & 15) != 0) return false;
+    for (int i = 0; i < d.nk; ++i)
+        if ((d.kst[i] * 4) % 16 != 0) return false;
+    return true;
+}
+
 constexpr bool rowst_type_ok(int op, int cd) { return op == OP_ADD && (cd == DT_F32 || cd == DT_F64); }
 constexpr bool rowco_type_ok(int op, int cd) {
     const bool w48 = cd == DT_I32 || cd == DT_I64 || cd == DT_U32 || cd == DT_U64 || cd == DT_F32 || cd == DT_F64;
@@ -767,7 +965,7 @@ inline bool row_narrow_ok(const RedDesc& d, int es) {
     if (d.ws != 1 || d.adt != d.cd || d.K != 0 || d.nk != 1 || d.kst[0] != d.w) return false;
     const int64_t rb = d.w * es;
     if (rb % 16 != 0 || rb < 16 || rb > NAR_MAXROWB) return false;
-    return (reinterpret_cast<uintptr_t>(d.a) & 15) == 0 && d.nout >= 148 * 256;
+    return (reinterpret_cast<uintptr_t>(d.a) & 15) == 0 && d.nout >= sm_count() * 256;
 }
 constexpr bool rownar_type_ok(int op, int cd) { return rowst_type_ok(op, cd) || rowco_type_ok(op, cd); }
 
@@ -780,11 +978,26 @@ static cudaError_t launch_row_wide(const RedDesc& din, cudaStream_t s) {
         if (row_narrow_ok(din, (int)sizeof(T))) {
             const int64_t R = std::min<int64_t>(2048, (NAR_WIN_BYTES / 16) / (din.w * (int64_t)sizeof(T) / 16));
             const int64_t nwin = (din.nout + R - 1) / R;
-            const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(nwin, 148LL * NAR_CTAS));
+            const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(nwin, (int64_t)sm_count() * NAR_CTAS));
             auto k = k_red_rownar<OP, CD>;
             const size_t smem = (size_t)NAR_STAGES * NAR_WIN_BYTES;
             cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
             k<<<grid, RED_THREADS, smem, s>>>(din);
+            count_launch();
+            return cudaGetLastError();
+        }
+    }
+    if constexpr (OP == OP_ADD && CD == DT_F32) {
+        if (pw32_ok(din)) {
+            auto k = k_red_pw32<OP, CD>;
+            cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)PW32_SMEM);
+            if (e != cudaSuccess) return e;
+            int per_sm = 1;
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, 32 * PW32_WARPS, PW32_SMEM);
+            const int64_t units = din.nout << din.K;
+            const int64_t ctas = (units + PW32_WARPS - 1) / PW32_WARPS;
+            const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(ctas, (int64_t)sm_count() * std::max(per_sm, 1)));
+            k<<<grid, 32 * PW32_WARPS, PW32_SMEM, s>>>(din);
             count_launch();
             return cudaGetLastError();
         }
@@ -800,14 +1013,14 @@ static cudaError_t launch_row_wide(const RedDesc& din, cudaStream_t s) {
         int per_sm = 1;
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, 32 * rst_warps<T>(), smem);
         const int64_t ctas = (units + rst_warps<T>() - 1) / rst_warps<T>();
-        const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(ctas, 148LL * std::max(per_sm, 1)));
+        const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(ctas, (int64_t)sm_count() * std::max(per_sm, 1)));
         k<<<grid, 32 * rst_warps<T>(), smem, s>>>(d);
         count_launch();
         return cudaGetLastError();
     } else if constexpr (rowco_type_ok(OP, CD)) {
         if (!row_wide_ok(din, (int)sizeof(T))) return cudaErrorNotSupported;
         const int64_t units = din.nout << din.K;
-        const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(units, 148LL * RCO_CTAS));
+        const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(units, (int64_t)sm_count() * RCO_CTAS));
         k_red_rowco<OP, CD><<<grid, RED_THREADS, 0, s>>>(din);
         count_launch();
         return cudaGetLastError();

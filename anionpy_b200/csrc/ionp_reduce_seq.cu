@@ -6,7 +6,7 @@ namespace ionp {
 static int seq_grid(int64_t nout, int threads) {
     int64_t g = (nout + threads - 1) / threads;
     if (g < 1) g = 1;
-    if (g > 148 * 16) g = 148 * 16;
+    if (g > sm_count() * 16) g = sm_count() * 16;
     return (int)g;
 }
 
@@ -29,7 +29,7 @@ static cudaError_t col_staged(const RedDesc& d, cudaStream_t s) {
     auto k = k_red_col_staged<OPV, D>;
     cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     const int64_t tiles = (d.kshape[0] + colst_cols<T>() - 1) / colst_cols<T>();
-    const int64_t cap = 148LL * COLST_CTAS;
+    const int64_t cap = (int64_t)sm_count() * COLST_CTAS;
     int grid = (int)(tiles < cap ? tiles : cap);
     k<<<grid, RED_THREADS, smem, s>>>(d);
     count_launch();
@@ -91,7 +91,7 @@ template <int OPV>
 static cudaError_t col_split_op(const RedDesc& d, cudaStream_t s) {
     const int64_t ntask = d.nout << d.K;
     int64_t g = (ntask + RED_THREADS - 1) / RED_THREADS;
-    if (g > 148 * 8) g = 148 * 8;
+    if (g > sm_count() * 8) g = sm_count() * 8;
     const int grid = (int)(g < 1 ? 1 : g);
 #define IONP_DTCASE(D)                                                  \
     case D:                                                             \

@@ -110,29 +110,40 @@ __device__ __forceinline__ double x_sqrt(double x) { return isnan_d(x) ? quiet_d
 // is within a factor two of y, so Sterbenz applies), and adding y back with
 // x's sign repairs the one-too-large case exactly. Larger quotients take the
 // library's fmod.
-__device__ __forceinline__ float x_fmod(float x, float y) {
+// the special values and the huge-quotient case, out of line
+static __device__ __noinline__ float x_fmod_full(float x, float y) {
     if (isnan_f(x) || isnan_f(y)) return nan2(x, y);
     if (isinf(x) || y == 0.0f) return dnan_f();
     if (isinf(y)) return x;
-    const float q = truncf(__fdiv_rn(x, y));
-    if (fabsf(q) < 0x1p23f) {
-        float r = __fmaf_rn(-q, y, x);
-        if (r != 0.0f && signbit(r) != signbit(x)) r = __fadd_rn(r, copysignf(y, x));
-        return r == 0.0f ? copysignf(0.0f, x) : r;
-    }
     return fmodf(x, y);
 }
-__device__ __forceinline__ double x_fmod(double x, double y) {
+static __device__ __noinline__ double x_fmod_full(double x, double y) {
     if (isnan_d(x) || isnan_d(y)) return nan2(x, y);
     if (isinf(x) || y == 0.0) return dnan_d();
     if (isinf(y)) return x;
-    const double q = trunc(__ddiv_rn(x, y));
-    if (fabs(q) < 0x1p52) {
-        double r = __fma_rn(-q, y, x);
-        if (r != 0.0 && signbit(r) != signbit(x)) r = __dadd_rn(r, copysign(y, x));
-        return r == 0.0 ? copysign(0.0, x) : r;
-    }
     return fmod(x, y);
+}
+__device__ __forceinline__ float x_fmod(float x, float y) {
+    if (isfinite(x) && isfinite(y) && y != 0.0f) {
+        const float q = truncf(__fdiv_rn(x, y));
+        if (fabsf(q) < 0x1p23f) {
+            float r = __fmaf_rn(-q, y, x);
+            if (r != 0.0f && signbit(r) != signbit(x)) r = __fadd_rn(r, copysignf(y, x));
+            return r == 0.0f ? copysignf(0.0f, x) : r;
+        }
+    }
+    return x_fmod_full(x, y);
+}
+__device__ __forceinline__ double x_fmod(double x, double y) {
+    if (isfinite(x) && isfinite(y) && y != 0.0) {
+        const double q = trunc(__ddiv_rn(x, y));
+        if (fabs(q) < 0x1p52) {
+            double r = __fma_rn(-q, y, x);
+            if (r != 0.0 && signbit(r) != signbit(x)) r = __dadd_rn(r, copysign(y, x));
+            return r == 0.0 ? copysign(0.0, x) : r;
+        }
+    }
+    return x_fmod_full(x, y);
 }
 
 // ---------------------------------------------------------------------------
@@ -378,19 +389,39 @@ template <> struct FOps<DT_F16> {
 };
 
 // float floor_divide in numpy's npy_divmod order (ufunc.rs:2493-2572).
-template <int D> __device__ __forceinline__ typename FOps<D>::T float_floor_divide(typename FOps<D>::T x, typename FOps<D>::T y) {
+// floor_divide_full is the whole sequence, special values included; it is
+// kept out of line so that the unrolled element loops carry only the fast
+// path below (its code would otherwise be copied into every unrolled
+// element and overflow the instruction cache).
+template <int D> static __device__ __noinline__ typename FOps<D>::T floor_divide_full(typename FOps<D>::T x, typename FOps<D>::T y) {
     typedef FOps<D> O;
     typedef typename O::T T;
     if (O::isinf_(x) && O::isfin(y) && !O::iszero(y)) return O::nan();
     if (O::isinf_(y) && O::isfin(x) && !O::iszero(x) && O::neg(x) != O::neg(y)) return O::negone();
     if (O::isfin(x) && O::isfin(y) && !O::iszero(y)) {
-        if constexpr (D == DT_F32 || D == DT_F64) {
-            // One division: with t = trunc(fl(x / y)) below 2^20 (2^49),
-            // x - t*y is exact in one FMA, one repair step makes t the exact
-            // truncated quotient q and r = fmod(x, y), and npy_divmod's
-            // (x - r) / y then lies within 1/4 of q, so its floor-and-round
-            // gives q (q - 1 after the sign fix) exactly; a zero result takes
-            // npy_divmod's copysign(0, x / y), the sign of x XOR y.
+        T raw_r = O::rem(x, y);
+        T div = O::div(O::sub(x, raw_r), y);
+        if (!O::iszero(raw_r) && O::neg(raw_r) != O::neg(y)) div = O::sub(div, O::one());
+        if (!O::iszero(div)) {
+            T fl = O::floor_(div);
+            return O::gt(O::sub(div, fl), O::half()) ? O::add(fl, O::one()) : fl;
+        }
+        return O::copysign0(O::div(x, y));
+    }
+    return O::floor_(O::div(x, y));
+}
+template <int D> __device__ __forceinline__ typename FOps<D>::T float_floor_divide(typename FOps<D>::T x, typename FOps<D>::T y) {
+    typedef FOps<D> O;
+    typedef typename O::T T;
+    if constexpr (D == DT_F32 || D == DT_F64) {
+        // One division: with x, y finite, y != 0 and t = trunc(fl(x / y))
+        // below 2^20 (2^49), x - t*y is exact in one FMA, one repair step
+        // makes t the exact truncated quotient q and r = fmod(x, y), and
+        // npy_divmod's (x - r) / y then lies within 1/4 of q, so its
+        // floor-and-round gives q (q - 1 after the sign fix) exactly; a
+        // zero result takes npy_divmod's copysign(0, x / y), the sign of x
+        // XOR y. Everything else takes the full sequence.
+        if (O::isfin(x) && O::isfin(y) && !O::iszero(y)) {
             const T t = trunc(O::div(x, y));
             if (fabs(t) < (D == DT_F32 ? (T)0x1p20 : (T)0x1p49)) {
                 T r, q = t;
@@ -405,16 +436,8 @@ template <int D> __device__ __forceinline__ typename FOps<D>::T float_floor_divi
                 return q;
             }
         }
-        T raw_r = O::rem(x, y);
-        T div = O::div(O::sub(x, raw_r), y);
-        if (!O::iszero(raw_r) && O::neg(raw_r) != O::neg(y)) div = O::sub(div, O::one());
-        if (!O::iszero(div)) {
-            T fl = O::floor_(div);
-            return O::gt(O::sub(div, fl), O::half()) ? O::add(fl, O::one()) : fl;
-        }
-        return O::copysign0(O::div(x, y));
     }
-    return O::floor_(O::div(x, y));
+    return floor_divide_full<D>(x, y);
 }
 
 // float_max / float_min (ufunc.rs:2402-2436)

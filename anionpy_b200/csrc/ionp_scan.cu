@@ -177,7 +177,7 @@ template <int OP, int CD> constexpr bool scan_valid() {
 
 inline int sc_grid(int64_t items) {
     int64_t g = (items + SC_THREADS - 1) / SC_THREADS;
-    return (int)std::max<int64_t>(1, std::min<int64_t>(g, 148LL * 8));
+    return (int)std::max<int64_t>(1, std::min<int64_t>(g, (int64_t)sm_count() * 8));
 }
 
 template <int OP, int CD>
@@ -303,8 +303,8 @@ int32_t fiber_call(int mode, int32_t op, const IonpArr* a, int32_t axis, const i
     // associative folds over few long fibers: parts of >= 1024 elements,
     // enough (fiber, part) threads for every SM
     void* carry = nullptr;
-    if (mode == 0 && d.nfib < 148 * 256 && len >= 4096) {
-        int64_t parts = std::min<int64_t>(len / 1024, (148LL * 1024 + d.nfib - 1) / d.nfib);
+    if (mode == 0 && d.nfib < sm_count() * 256 && len >= 4096) {
+        int64_t parts = std::min<int64_t>(len / 1024, ((int64_t)sm_count() * 1024 + d.nfib - 1) / d.nfib);
         if (parts > 1) {
             d.parts = parts;
             carry = scratch_alloc((size_t)(d.nfib * parts) * 8 + 64, s);
@@ -347,4 +347,389 @@ extern "C" int32_t ionp_reduceat(int32_t op, const IonpArr* a, int32_t axis, con
                                  IonpArr* out, IonpStream stream) {
     if (nindices < 0 || (nindices > 0 && !indices)) return set_err(IONP_ERR_INVALID, "bad indices");
     return fiber_call(1, op, a, axis, indices, nindices, out, "reduceat", (cudaStream_t)stream);
+}
+
+namespace ionp {
+
+// ---------------------------------------------------------------------------
+// ufunc.at: target[idx_i, ...] = op(target[idx_i, ...], values[i, ...]) for
+// i in order (at_binary, ionp-core/src/ufunc.rs:9577-9733). Repeated indices
+// apply in order, so each distinct row is one chain: the host groups the
+// index positions by row (first occurrence order of rows, positions
+// ascending within a row) and one thread takes one (row, element) pair,
+// folding the row's values in order in the compute dtype CD:
+//  * logical ops: CD bool (the target element read as bool, the result
+//    written back as 0/1 of the target dtype);
+//  * comparisons: CD the target dtype, the bool result written back as
+//    0/1 of it after every step;
+//  * other ops: CD = the ufunc's result dtype for (target, values); when it
+//    differs from the target's, the reference casts the whole target to CD,
+//    applies the updates, and casts the whole target back, so every element
+//    makes the round trip (done by the host as two casts before this
+//    kernel); the updates then chain in CD and are cast back once.
+// ---------------------------------------------------------------------------
+struct AtDesc {
+    void* t;                        // target row 0, element 0
+    int32_t tdt;
+    int64_t tst0;                   // target stride along axis 0
+    const void* v;                  // values, broadcast to (n, row...)
+    int32_t vdt;
+    int64_t vst0;
+    int32_t nr;                     // row dims (merged)
+    int64_t rshape[SC_MAXD], rtst[SC_MAXD], rvst[SC_MAXD];
+    int64_t rown;                   // elements per row
+    int64_t nrows;                  // distinct rows
+    const int64_t* row;             // [nrows] target row index
+    const int64_t* start;           // [nrows + 1] into pos
+    const int64_t* pos;             // value positions, grouped by row
+};
+
+template <int CD> __device__ __forceinline__ typename DT<CD>::T from_bool(bool b) {
+    if constexpr (CD == DT_F16) return b ? (uint16_t)0x3C00 : (uint16_t)0;
+    else return (typename DT<CD>::T)(b ? 1 : 0);
+}
+
+template <int OP, int CD>
+__global__ void __launch_bounds__(SC_THREADS) k_at(AtDesc d) {
+    typedef typename DT<CD>::T T;
+    const int64_t n = d.nrows * d.rown, stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += stride) {
+        const int64_t r = t / d.rown;
+        int64_t e = t - r * d.rown, to = 0, vo = 0;
+        for (int k = d.nr - 1; k >= 0; --k) {
+            const int64_t q = e / d.rshape[k], i = e - q * d.rshape[k];
+            e = q;
+            to += i * d.rtst[k];
+            vo += i * d.rvst[k];
+        }
+        const int64_t tp = d.row[r] * d.tst0 + to;
+        T acc = load_cast<CD>(d.t, tp, d.tdt);
+        for (int64_t k = d.start[r]; k < d.start[r + 1]; ++k) {
+            const T x = load_cast<CD>(d.v, d.pos[k] * d.vst0 + vo, d.vdt);
+            if constexpr (op_is_compare(OP)) acc = from_bool<CD>((bool)BinOp<OP, CD>::apply(acc, x));
+            else acc = (T)BinOp<OP, CD>::apply(acc, x);
+        }
+        store_cast<CD>(d.t, tp, d.tdt, acc);
+    }
+}
+
+template <int OP, int CD> constexpr bool at_valid() {
+    if (op_is_logical(OP)) return CD == DT_BOOL;
+    if (op_is_compare(OP)) return true;
+    if constexpr (bin_valid<OP, CD>()) return BinOp<OP, CD>::OUT_DT == CD;
+    return false;
+}
+
+template <int OP>
+cudaError_t at_op(int cd, const AtDesc& d, cudaStream_t s) {
+#define IONP_CASE(D)                                                                              \
+    case D:                                                                                       \
+        if constexpr (at_valid<OP, D>()) {                                                        \
+            k_at<OP, D><<<sc_grid(d.nrows * d.rown), SC_THREADS, 0, s>>>(d);                      \
+            count_launch();                                                                       \
+            return cudaGetLastError();                                                            \
+        }                                                                                         \
+        break;
+    switch (cd) {
+        IONP_CASE(DT_BOOL) IONP_CASE(DT_I8) IONP_CASE(DT_I16) IONP_CASE(DT_I32) IONP_CASE(DT_I64)
+        IONP_CASE(DT_U8) IONP_CASE(DT_U16) IONP_CASE(DT_U32) IONP_CASE(DT_U64)
+        IONP_CASE(DT_F16) IONP_CASE(DT_F32) IONP_CASE(DT_F64)
+    }
+#undef IONP_CASE
+    return cudaErrorInvalidValue;
+}
+
+cudaError_t launch_at(int op, int cd, const AtDesc& d, cudaStream_t s) {
+    switch (op) {
+        case OP_ADD: return at_op<OP_ADD>(cd, d, s);
+        case OP_SUBTRACT: return at_op<OP_SUBTRACT>(cd, d, s);
+        case OP_MULTIPLY: return at_op<OP_MULTIPLY>(cd, d, s);
+        case OP_DIVIDE: return at_op<OP_DIVIDE>(cd, d, s);
+        case OP_MAXIMUM: return at_op<OP_MAXIMUM>(cd, d, s);
+        case OP_MINIMUM: return at_op<OP_MINIMUM>(cd, d, s);
+        case OP_GREATER: return at_op<OP_GREATER>(cd, d, s);
+        case OP_GREATER_EQUAL: return at_op<OP_GREATER_EQUAL>(cd, d, s);
+        case OP_LESS: return at_op<OP_LESS>(cd, d, s);
+        case OP_LESS_EQUAL: return at_op<OP_LESS_EQUAL>(cd, d, s);
+        case OP_EQUAL: return at_op<OP_EQUAL>(cd, d, s);
+        case OP_NOT_EQUAL: return at_op<OP_NOT_EQUAL>(cd, d, s);
+        case OP_LOGICAL_AND: return at_op<OP_LOGICAL_AND>(cd, d, s);
+        case OP_LOGICAL_OR: return at_op<OP_LOGICAL_OR>(cd, d, s);
+        case OP_LOGICAL_XOR: return at_op<OP_LOGICAL_XOR>(cd, d, s);
+        case OP_BITWISE_AND: return at_op<OP_BITWISE_AND>(cd, d, s);
+        case OP_BITWISE_OR: return at_op<OP_BITWISE_OR>(cd, d, s);
+        case OP_BITWISE_XOR: return at_op<OP_BITWISE_XOR>(cd, d, s);
+        case OP_FLOOR_DIVIDE: return at_op<OP_FLOOR_DIVIDE>(cd, d, s);
+        case OP_LEFT_SHIFT: return at_op<OP_LEFT_SHIFT>(cd, d, s);
+        case OP_RIGHT_SHIFT: return at_op<OP_RIGHT_SHIFT>(cd, d, s);
+        case OP_REMAINDER: return at_op<OP_REMAINDER>(cd, d, s);
+        case OP_FMOD: return at_op<OP_FMOD>(cd, d, s);
+    }
+    return cudaErrorInvalidValue;
+}
+
+// Unary .at (at_unary, ufunc.rs:9301; at_math_unary, ufunc.rs:9805): every
+// occurrence of a row applies op once more to its elements, each time
+// computed in CD and written back in the target's dtype (logical_not: CD
+// bool, the target read as bool).
+template <int OP, int CD>
+__global__ void __launch_bounds__(SC_THREADS) k_at_unary(AtDesc d) {
+    typedef UnOp<OP, CD> U;
+    const int64_t n = d.nrows * d.rown, stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += stride) {
+        const int64_t r = t / d.rown;
+        int64_t e = t - r * d.rown, to = 0;
+        for (int k = d.nr - 1; k >= 0; --k) {
+            const int64_t q = e / d.rshape[k], i = e - q * d.rshape[k];
+            e = q;
+            to += i * d.rtst[k];
+        }
+        const int64_t tp = d.row[r] * d.tst0 + to, c = d.start[r + 1] - d.start[r];
+        for (int64_t k = 0; k < c; ++k) store_cast<U::OUT_DT>(d.t, tp, d.tdt, U::apply(load_cast<CD>(d.t, tp, d.tdt)));
+    }
+}
+
+template <int OP>
+cudaError_t at_un_op(int cd, const AtDesc& d, cudaStream_t s) {
+    constexpr bool MATH = OP >= OP_SQRT;
+#define IONP_CASE(D)                                                                              \
+    case D:                                                                                       \
+        if constexpr (!MATH || dt_is_float(D)) {                                                  \
+            k_at_unary<OP, D><<<sc_grid(d.nrows * d.rown), SC_THREADS, 0, s>>>(d);                \
+            count_launch();                                                                       \
+            return cudaGetLastError();                                                            \
+        }                                                                                         \
+        break;
+    switch (cd) {
+        IONP_CASE(DT_BOOL) IONP_CASE(DT_I8) IONP_CASE(DT_I16) IONP_CASE(DT_I32) IONP_CASE(DT_I64)
+        IONP_CASE(DT_U8) IONP_CASE(DT_U16) IONP_CASE(DT_U32) IONP_CASE(DT_U64)
+        IONP_CASE(DT_F16) IONP_CASE(DT_F32) IONP_CASE(DT_F64)
+    }
+#undef IONP_CASE
+    return cudaErrorInvalidValue;
+}
+
+cudaError_t launch_at_unary(int op, int cd, const AtDesc& d, cudaStream_t s) {
+    switch (op) {
+        case OP_NEGATIVE: return at_un_op<OP_NEGATIVE>(cd, d, s);
+        case OP_ABSOLUTE: return at_un_op<OP_ABSOLUTE>(cd, d, s);
+        case OP_INVERT: return at_un_op<OP_INVERT>(cd, d, s);
+        case OP_LOGICAL_NOT: return at_un_op<OP_LOGICAL_NOT>(cd, d, s);
+        case OP_SQRT: return at_un_op<OP_SQRT>(cd, d, s);
+        case OP_EXP: return at_un_op<OP_EXP>(cd, d, s);
+        case OP_LOG: return at_un_op<OP_LOG>(cd, d, s);
+        case OP_SIN: return at_un_op<OP_SIN>(cd, d, s);
+    }
+    return cudaErrorInvalidValue;
+}
+
+// [lo, hi) bytes an array's elements can touch
+static void byte_span(const IonpArr* a, uintptr_t* lo, uintptr_t* hi) {
+    const int64_t b = dt_bytes(a->dtype);
+    int64_t mn = 0, mx = 0;
+    for (int i = 0; i < a->ndim; ++i) {
+        const int64_t ext = (a->shape[i] - 1) * a->strides[i];
+        if (ext < 0) mn += ext; else mx += ext;
+    }
+    const uintptr_t base = (uintptr_t)elem_ptr(a);
+    *lo = base + mn * b;
+    *hi = base + (mx + 1) * b;
+}
+
+static IonpArr c_contig_like(const IonpArr* a, int dtype, void* data) {
+    IonpArr r;
+    memset(&r, 0, sizeof(r));
+    r.dtype = dtype;
+    r.ndim = a->ndim;
+    int64_t acc = 1;
+    for (int i = a->ndim - 1; i >= 0; --i) {
+        r.shape[i] = a->shape[i];
+        r.strides[i] = acc;
+        acc *= a->shape[i] > 0 ? a->shape[i] : 1;
+    }
+    r.data = data;
+    return r;
+}
+
+// One .at pass over `t` (already in its compute dtype unless comparisons /
+// logical ops, which the kernel casts per element).
+static int32_t at_pass(int32_t op, int cd, bool unary, const IonpArr* t, const IonpArr* v, const int64_t* vst,
+                       const std::vector<int64_t>& rows, cudaStream_t s) {
+    const int nd = t->ndim;
+    if (rows.empty()) return IONP_OK;
+    // group index positions by row: rows ascending, positions ascending
+    std::vector<int64_t> order(rows.size());
+    for (size_t i = 0; i < order.size(); ++i) order[i] = (int64_t)i;
+    std::stable_sort(order.begin(), order.end(), [&](int64_t x, int64_t y) { return rows[x] < rows[y]; });
+    std::vector<int64_t> urow, start;
+    for (size_t i = 0; i < order.size(); ++i) {
+        if (i == 0 || rows[order[i]] != rows[order[i - 1]]) {
+            urow.push_back(rows[order[i]]);
+            start.push_back((int64_t)i);
+        }
+    }
+    start.push_back((int64_t)order.size());
+    const int64_t G = (int64_t)urow.size();
+    // row dims: unit dims dropped, neighbours merged when both strides chain
+    struct RD { int64_t n, ts, vs; };
+    std::vector<RD> rd;
+    int64_t rown = 1;
+    for (int i = 1; i < nd; ++i) {
+        rown *= t->shape[i];
+        if (t->shape[i] == 1) continue;
+        RD x{t->shape[i], t->strides[i], v ? vst[i] : 0};
+        if (!rd.empty() && rd.back().ts == x.ts * x.n && rd.back().vs == x.vs * x.n) {
+            rd.back().n *= x.n; rd.back().ts = x.ts; rd.back().vs = x.vs;
+            continue;
+        }
+        rd.push_back(x);
+    }
+    if (rown == 0) return IONP_OK;
+    std::vector<int64_t> host;
+    host.reserve(urow.size() + start.size() + order.size());
+    host.insert(host.end(), urow.begin(), urow.end());
+    host.insert(host.end(), start.begin(), start.end());
+    host.insert(host.end(), order.begin(), order.end());
+    int64_t* dev = (int64_t*)scratch_alloc(host.size() * 8, s);
+    if (!dev) return IONP_ERR_OOM;
+    int32_t st = cuda_err(cudaMemcpyAsync(dev, host.data(), host.size() * 8, cudaMemcpyHostToDevice, s), "at indices");
+    AtDesc d;
+    memset(&d, 0, sizeof(d));
+    d.tdt = t->dtype;
+    d.tst0 = nd ? t->strides[0] : 0;
+    d.vdt = v ? v->dtype : 0;
+    d.vst0 = (v && nd) ? vst[0] : 0;
+    d.row = dev;
+    d.start = dev + G;
+    d.pos = dev + 2 * G + 1;
+    d.nrows = G;
+    const int lead = (int)rd.size() > SC_MAXD ? (int)rd.size() - SC_MAXD : 0;
+    d.nr = (int)rd.size() - lead;
+    d.rown = 1;
+    for (int i = 0; i < d.nr; ++i) {
+        d.rshape[i] = rd[lead + i].n; d.rtst[i] = rd[lead + i].ts; d.rvst[i] = rd[lead + i].vs;
+        d.rown *= d.rshape[i];
+    }
+    int64_t nlead = 1;
+    for (int i = 0; i < lead; ++i) nlead *= rd[i].n;
+    for (int64_t q = 0; q < nlead && !st; ++q) {
+        int64_t rem = q, ot = 0, ov = 0;
+        for (int i = lead - 1; i >= 0; --i) {
+            const int64_t id = rem % rd[i].n;
+            rem /= rd[i].n;
+            ot += id * rd[i].ts;
+            ov += id * rd[i].vs;
+        }
+        d.t = (char*)elem_ptr(t) + ot * dt_bytes(t->dtype);
+        d.v = v ? elem_ptr(v) + ov * dt_bytes(v->dtype) : nullptr;
+        st = cuda_err(unary ? launch_at_unary(op, cd, d, s) : launch_at(op, cd, d, s), "at launch");
+    }
+    scratch_free(dev, s);
+    return st;
+}
+
+}  // namespace ionp
+
+extern "C" int32_t ionp_at(int32_t op, IonpArr* target, const int64_t* indices, int64_t nindices,
+                           const IonpArr* values, IonpStream stream) {
+    int32_t st;
+    if ((st = check_arr(target, "target"))) return st;
+    if (values && (st = check_arr(values, "values"))) return st;
+    if (nindices < 0 || (nindices > 0 && !indices)) return set_err(IONP_ERR_INVALID, "bad indices");
+    cudaStream_t s = (cudaStream_t)stream;
+    const bool unary = op >= OP_NEGATIVE && op <= OP_SIN;
+    const bool math_un = op >= OP_SQRT && op <= OP_SIN;
+    if (!unary && !(op >= OP_ADD && op <= OP_RIGHT_SHIFT) && op != OP_REMAINDER && op != OP_FMOD)
+        return set_err(IONP_ERR_UNSUPPORTED, std::string("op ") + std::to_string(op) + " has no .at in this engine");
+    if (unary && values) return set_err(IONP_ERR_INVALID, "unary ufunc .at() takes no third argument");
+    if (!unary && !values) return set_err(IONP_ERR_INVALID, "binary ufunc .at() requires a values argument");
+    const int tdt = target->dtype;
+    int cd = 0, rd = 0;
+    if (math_un && (st = unary_loop(op, tdt, &cd, &rd))) return st;   // checked before the indices
+    // normalize_at_indices (ufunc.rs:9250)
+    const int nd = target->ndim;
+    std::vector<int64_t> rows;
+    if (nd == 0) {
+        if (nindices)
+            return set_err(IONP_ERR_INDEX, "too many indices for array: array is 0-dimensional, but " +
+                                               std::to_string(nindices) + " were indexed");
+        rows.push_back(0);
+    } else {
+        const int64_t n = target->shape[0];
+        rows.resize((size_t)nindices);
+        for (int64_t i = 0; i < nindices; ++i) {
+            const int64_t x = indices[i], y = x < 0 ? x + n : x;
+            if (y < 0 || y >= n)
+                return set_err(IONP_ERR_INDEX, "index " + std::to_string(x) + " is out of bounds for axis 0 with size " +
+                                                   std::to_string(n));
+            rows[i] = y;
+        }
+    }
+    bool slow = false;
+    if (unary) {
+        if (op == OP_LOGICAL_NOT) cd = DT_BOOL;
+        else if (!math_un) {
+            if ((st = unary_loop(op, tdt, &cd, &rd))) return st;
+            if (rd != tdt)
+                return set_err(IONP_ERR_TYPE, std::string("'.at' would change dtype from ") + dt_name(tdt) + " to " +
+                                                  dt_name(rd) + ", which is not supported");
+        }
+    } else if (op_is_logical(op)) {
+        cd = DT_BOOL;
+    } else if (op_is_compare(op)) {
+        if (!dt_valid(values->dtype) || !dt_valid(tdt)) return set_err(IONP_ERR_UNSUPPORTED, "unsupported dtype");
+        cd = tdt;
+    } else {
+        if ((st = binary_loop(op, tdt, values->dtype, &cd, &rd))) return st;
+        cd = rd;
+        slow = cd != tdt;
+    }
+    // values broadcast against (len(indices),) + row shape as a whole
+    int64_t vshape[IONP_MAX_DIMS], vst[IONP_MAX_DIMS];
+    int vnd = 0;
+    if (!unary) {
+        if (nd) {
+            vshape[0] = nindices;
+            for (int i = 1; i < nd; ++i) vshape[i] = target->shape[i];
+            vnd = nd;
+        }
+        if (!bcast_strides(values, vnd, vshape, vst))
+            return set_err(IONP_ERR_BROADCAST, "array is not broadcastable to correct shape");
+        if (!nd) vst[0] = 0;
+    }
+    if (numel(target) == 0) return IONP_OK;
+    if (slow) {
+        // compute on a whole-target copy in the promoted dtype, then cast
+        // every element back (the reference's round trip)
+        void* buf = scratch_alloc((size_t)numel(target) * dt_bytes(cd), s);
+        if (!buf) return IONP_ERR_OOM;
+        IonpArr tmp = c_contig_like(target, cd, buf);
+        st = cast_impl(target, &tmp, nullptr, s);
+        if (!st) st = at_pass(op, cd, false, &tmp, values, vst, rows, s);
+        if (!st) st = cast_impl(&tmp, target, nullptr, s);
+        scratch_free(buf, s);
+        return st;
+    }
+    // values that share memory with the target are read as they were
+    // before the call: take a copy first
+    void* vcopy = nullptr;
+    IonpArr vc;
+    const IonpArr* vv = values;
+    if (values && numel(values) > 0) {
+        uintptr_t tl, th, vl, vh;
+        byte_span(target, &tl, &th);
+        byte_span(values, &vl, &vh);
+        if (vl < th && tl < vh) {
+            vcopy = scratch_alloc((size_t)numel(values) * dt_bytes(values->dtype), s);
+            if (!vcopy) return IONP_ERR_OOM;
+            vc = c_contig_like(values, values->dtype, vcopy);
+            if ((st = cast_impl(values, &vc, nullptr, s))) { scratch_free(vcopy, s); return st; }
+            if (!bcast_strides(&vc, vnd, vshape, vst)) { scratch_free(vcopy, s); return set_err(IONP_ERR_BROADCAST, "array is not broadcastable to correct shape"); }
+            if (!nd) vst[0] = 0;
+            vv = &vc;
+        }
+    }
+    st = at_pass(op, cd, unary, target, vv, vst, rows, s);
+    if (vcopy) scratch_free(vcopy, s);
+    return st;
 }

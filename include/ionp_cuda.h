@@ -201,6 +201,21 @@ int32_t ionp_accumulate(int32_t op, const IonpArr* a, int32_t axis, IonpArr* out
  * IONP_ERR_INDEX. out: a's shape with the axis extent nindices. */
 int32_t ionp_reduceat(int32_t op, const IonpArr* a, int32_t axis, const int64_t* indices, int64_t nindices,
                       IonpArr* out, IonpStream stream);
+/* ufunc.at, in place on `target`: at_binary (ufunc.rs:9577),
+ * at_math_binary (ufunc.rs:9932; remainder, fmod), at_unary (ufunc.rs:9301)
+ * and at_math_unary (ufunc.rs:9805). For i in order,
+ * target[indices[i], ...] = op(target[indices[i], ...], values[i, ...]),
+ * values broadcast against (nindices,) + target.shape[1:] as a whole;
+ * repeated indices apply in order; computed in the target's dtype
+ * (comparisons: 0/1 of it; logical ops: in bool) or, when the ufunc
+ * promotes, on a whole-target copy in the promoted dtype that is cast back
+ * element by element. Unary ops (values NULL) apply once per occurrence.
+ * indices: HOST int64, negative counts from the end, each within axis 0
+ * (a 0-d target takes nindices = 0 and applies once), else IONP_ERR_INDEX.
+ * Values that share memory with the target are read as they were before
+ * the call. No FPE report (the reference's .at has none). */
+int32_t ionp_at(int32_t op, IonpArr* target, const int64_t* indices, int64_t nindices, const IonpArr* values,
+                IonpStream stream);
 /* argmin (is_max=0) / argmax (is_max=1): argext (ufunc.rs:8131) behind
  * do_argext (ionp-py/src/reductions.rs:1198). axis = -1 means the flattened
  * C-order ravel (axis=None); out is int64 with the kept shape. */
@@ -292,10 +307,15 @@ int32_t ionp_mlp_train_step(IonpMlp* m, const float* x, const float* t, const fl
 
 /* ---------------------------------------------------------------- memory */
 /* Caching device allocator (the device counterpart of Buffer's Vec<T>,
- * ionp-core/src/buffer.rs:18): size-classed free lists, stream-ordered reuse. */
+ * ionp-core/src/buffer.rs:18): one pool per device (blocks are allocated
+ * on, and reused only on, the device current at ionp_alloc), size-classed
+ * free lists, stream-ordered reuse (a block freed on one stream is reused
+ * on another only after an event wait). A failed cudaMalloc releases the
+ * device's cached blocks and retries once, then returns IONP_ERR_OOM. */
 int32_t ionp_alloc(void** ptr, size_t bytes, IonpStream stream);
 int32_t ionp_free(void* ptr, IonpStream stream);
-/* bytes: [0] in use, [1] cached (free), [2] peak in use, [3] cudaMalloc calls */
+/* current device's pool, bytes: [0] in use, [1] cached (free), [2] peak in
+ * use, [3] cudaMalloc calls */
 int32_t ionp_alloc_stats(uint64_t* stats4);
 int32_t ionp_alloc_trim(void);
 

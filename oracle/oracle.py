@@ -376,3 +376,148 @@ def mean(a: np.ndarray, axis=None, dtype=None, keepdims=False, where=None):
     if keepdims:
         res = res.reshape([1 if i in axes else a.shape[i] for i in range(a.ndim)])
     return res, warned, cat
+
+
+def accumulate(op: str, a: np.ndarray, axis: int = 0):
+    """accumulate_axis (ionp-core/src/ufunc.rs:7967-8035, accumulate_axis_generic
+    7898): every fiber along `axis` folded left to right in the reduce-family
+    compute dtype, acc = x0, acc = op(acc, x_i) -- one oracle ufunc call per
+    step over all fibers at once (C-ordered result)."""
+    a = np.asarray(a)
+    cd = reduce_compute_dtype(op, a.dtype)
+    x = np.moveaxis(cast(np.ascontiguousarray(a), cd), axis, 0)
+    out = np.empty(x.shape, cd)
+    if x.shape[0] == 0:
+        return np.moveaxis(out, 0, axis)
+    acc = np.ascontiguousarray(x[0])
+    out[0, ...] = acc
+    for i in range(1, x.shape[0]):
+        acc = binary(op, acc, np.ascontiguousarray(x[i]))[0].astype(cd, copy=False).reshape(x.shape[1:])
+        out[i, ...] = acc
+    return np.ascontiguousarray(np.moveaxis(out, 0, axis))
+
+
+def reduceat(op: str, a: np.ndarray, indices, axis: int = 0):
+    """reduceat_binary_axis (ionp-core/src/ufunc.rs:8450, reduceat_axis_generic
+    8322): segment k folds x[idx_k .. idx_{k+1}) left to right (to the axis
+    end for the last), or is x[idx_k] alone when idx_{k+1} <= idx_k."""
+    a = np.asarray(a)
+    idx = [int(i) for i in np.asarray(indices).reshape(-1)]
+    n = a.shape[axis]
+    for i in idx:
+        if i < 0 or i >= n:
+            raise IndexError(f"index {i} out-of-bounds in {op}.reduceat [0, {n})")
+    cd = reduce_compute_dtype(op, a.dtype)
+    x = np.moveaxis(cast(np.ascontiguousarray(a), cd), axis, 0)
+    out = np.empty((len(idx),) + x.shape[1:], cd)
+    for k, start in enumerate(idx):
+        nxt = idx[k + 1] if k + 1 < len(idx) else n
+        acc = np.ascontiguousarray(x[start])
+        for j in range(start + 1, nxt):
+            acc = binary(op, acc, np.ascontiguousarray(x[j]))[0].astype(cd, copy=False).reshape(x.shape[1:])
+        out[k, ...] = acc
+    return np.ascontiguousarray(np.moveaxis(out, 0, axis))
+
+
+def outer(op: str, a: np.ndarray, b: np.ndarray):
+    """outer_binary (ionp-core/src/ufunc.rs:8212): op over the cross product,
+    shape a.shape + b.shape."""
+    a = np.asarray(a)
+    b = np.asarray(b)
+    return binary(op, a.reshape(a.shape + (1,) * b.ndim), b)[0]
+
+
+BINARY_AT_OPS = ("add", "subtract", "multiply", "divide", "maximum", "minimum", "greater", "greater_equal", "less",
+                 "less_equal", "equal", "not_equal", "logical_and", "logical_or", "logical_xor", "bitwise_and",
+                 "bitwise_or", "bitwise_xor", "floor_divide", "left_shift", "right_shift", "remainder", "fmod")
+LOGICAL = ("logical_and", "logical_or", "logical_xor")
+COMPARE = ("greater", "greater_equal", "less", "less_equal", "equal", "not_equal")
+
+
+def at_rows(shape, indices):
+    """normalize_at_indices (ionp-core/src/ufunc.rs:9250): negative indices
+    count from the end of axis 0; a 0-d target takes no index and applies
+    the op once."""
+    idx = [int(i) for i in np.asarray(indices, dtype=np.int64).reshape(-1)]
+    if len(shape) == 0:
+        if idx:
+            raise IndexError(f"too many indices for array: array is 0-dimensional, but {len(idx)} were indexed")
+        return [None]
+    n = shape[0]
+    rows = []
+    for i in idx:
+        j = i + n if i < 0 else i
+        if j < 0 or j >= n:
+            raise IndexError(f"index {i} is out of bounds for axis 0 with size {n}")
+        rows.append(j)
+    return rows
+
+
+def _cc(x):
+    """C-contiguous copy that keeps 0-d arrays 0-d."""
+    return np.array(x, order="C")
+
+
+def _row(t, r):
+    return t[...] if r is None else t[r, ...]
+
+
+def at(op: str, target: np.ndarray, indices, values=None):
+    """ufunc.at in place on the numpy array `target`: at_binary
+    (ionp-core/src/ufunc.rs:9577-9733), at_math_binary (9932), at_unary
+    (9301) and at_math_unary (9805), one oracle ufunc call per index:
+    * binary: values are broadcast against (len(indices),) + row shape as a
+      whole; logical ops compute in bool and store 0/1 of the target dtype;
+      comparisons compute in the target dtype (values cast to it) and store
+      0/1 of it; other ops compute in the target dtype, or, when the ufunc
+      promotes (target, values) to another dtype, on a whole-target copy in
+      that dtype cast back at the end;
+    * unary: logical_not in bool, stored back as 0/1; negative / absolute /
+      invert only where they keep the dtype (else TypeError "'.at' would
+      change dtype ..."); sqrt / exp / log / sin in their float loop dtype,
+      cast back after every application."""
+    dt = target.dtype
+    if values is None:
+        math = op in ("sqrt", "exp", "log", "sin")
+        if math:
+            unary_out_dtype(op, dt)          # checked before the indices
+        rows = at_rows(target.shape, indices)
+        if op == "logical_not":
+            for r in rows:
+                _row(target, r)[...] = cast(np.asarray(cast(_row(target, r), np.bool_) == 0), dt)
+            return target
+        if not math:
+            od = unary_out_dtype(op, dt)
+            if od != dt:
+                raise TypeError(f"'.at' would change dtype from {dt} to {od}, which is not supported")
+        for r in rows:
+            _row(target, r)[...] = cast(unary(op, _cc(_row(target, r)))[0], dt)
+        return target
+    values = np.asarray(values)
+    rows = at_rows(target.shape, indices)
+    vshape = ((len(rows),) + target.shape[1:]) if target.ndim else ()
+    if op in LOGICAL:
+        cd = np.dtype(np.bool_)
+    elif op in COMPARE:
+        cd = dt
+    else:
+        cd = binary_out_dtype(op, dt, values.dtype)
+        if cd != dt:
+            try:
+                np.broadcast_to(values, vshape)
+            except ValueError:
+                raise OracleError(1) from None
+            tmp = cast(_cc(target), cd)
+            at(op, tmp, indices, values)
+            target[...] = cast(tmp, dt)
+            return target
+    try:
+        v = np.broadcast_to(cast(_cc(values), cd), vshape)
+    except ValueError:
+        raise OracleError(1) from None
+    for i, r in enumerate(rows):
+        row = _cc(_row(target, r))
+        lhs = cast(row, cd) if op in LOGICAL else row
+        res = binary(op, lhs, _cc(v[i] if target.ndim else v))[0]
+        _row(target, r)[...] = cast(np.asarray(res), dt)
+    return target

@@ -3,7 +3,8 @@
 Inputs come from the reference's own differential corpus
 (Son0fSun/anionpy tests/differential/corpus.py: unary_corpus() and
 binary_corpus(), seed 20260731), imported at generation time from a local
-checkout of the reference (REFERENCE_ROOT, default /root/reference). The
+checkout of the reference, given as the first argument or in the
+REFERENCE_ROOT environment variable. The
 expected outputs are NumPy's, for the items the reference declares
 bit-exact against NumPy (tests/differential/r.json and the coverage ledger:
 add, subtract, multiply, divide, maximum, minimum, comparisons, logical and
@@ -11,8 +12,8 @@ bitwise ops, floor_divide, remainder, sum/add.reduce, maximum.reduce,
 argmin/argmax). Transcendentals are not pinned to NumPy here: on x86 NumPy's
 SIMD exp/log/sin differ from glibc, which is what the reference calls.
 
-Run:  python tests/golden/make_golden.py   (needs the reference checkout;
-the produced .npz files are committed and used without it.)
+Run:  python tests/golden/make_golden.py <reference checkout>
+(the produced .npz files are committed and used without it.)
 """
 from __future__ import annotations
 
@@ -24,7 +25,7 @@ import warnings
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REF = os.environ.get("REFERENCE_ROOT", "/root/reference")
+REF = None
 
 SUPPORTED = {np.dtype(t) for t in (np.bool_, np.int8, np.int16, np.int32, np.int64, np.uint8, np.uint16, np.uint32,
                                    np.uint64, np.float16, np.float32, np.float64)}
@@ -36,6 +37,10 @@ REDUCE = ["add", "maximum", "minimum", "multiply", "logical_and", "logical_or", 
 
 
 def main():
+    global REF
+    REF = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("REFERENCE_ROOT")
+    if not REF or not os.path.isdir(os.path.join(REF, "tests", "differential")):
+        sys.exit("usage: make_golden.py <reference checkout> (or set REFERENCE_ROOT)")
     sys.path.insert(0, os.path.join(REF, "tests", "differential"))
     import corpus  # the reference corpus builder (numpy only)
 

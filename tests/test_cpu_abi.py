@@ -153,3 +153,62 @@ def test_cast_scalar_matches_oracle():
                 got = out.view(np.uint8)[: np.dtype(dd).itemsize].view(dd)[0]
                 want = O.cast(src, dd).reshape(())[()]
                 assert np.array(got).tobytes() == np.array(want, dd).tobytes(), (sd, dd, v)
+
+
+def _arr(dtype=10, shape=(4,), strides=None, data=0x1000, ndim=None):
+    a = _lib.IonpArr()
+    a.dtype = dtype
+    a.ndim = len(shape) if ndim is None else ndim
+    for i, s in enumerate(shape[:32]):
+        a.shape[i] = s
+    st = strides or [1] * len(shape)
+    for i, s in enumerate(st[:32]):
+        a.strides[i] = s
+    a.offset = 0
+    a.data = data
+    return a
+
+
+BAD = {
+    "ndim > 32": (dict(ndim=33), _lib.ERR_INVALID, "ndim out of range"),
+    "negative ndim": (dict(ndim=-1), _lib.ERR_INVALID, "ndim out of range"),
+    "negative extent": (dict(shape=(4, -2)), _lib.ERR_INVALID, "negative extent"),
+    "NULL data": (dict(data=None), _lib.ERR_INVALID, "NULL data"),
+    "too many elements": (dict(shape=(1 << 40, 1 << 40)), _lib.ERR_INVALID, "2^62"),
+    "complex dtype": (dict(dtype=12), _lib.ERR_UNSUPPORTED, "not supported"),
+}
+
+
+@pytest.mark.parametrize("case", list(BAD))
+def test_malformed_descriptors_rejected_before_launch(case):
+    """Every compute entry point validates its descriptors on the host and
+    returns IONP_ERR_INVALID / IONP_ERR_UNSUPPORTED with a message, with no
+    CUDA call (this runs without a GPU)."""
+    L = _lib.load_library()
+    kw, want, msg = BAD[case]
+    bad, good = _arr(**kw), _arr()
+    P = ctypes.byref
+    calls = {
+        "ionp_binary": lambda: L.ionp_binary(0, P(bad), P(good), P(good), None, None, None),
+        "ionp_binary (out)": lambda: L.ionp_binary(0, P(good), P(good), P(bad), None, None, None),
+        "ionp_unary": lambda: L.ionp_unary(81, P(bad), P(good), None, None, None),
+        "ionp_cast": lambda: L.ionp_cast(P(bad), P(good), None),
+        "ionp_astype": lambda: L.ionp_astype(P(bad), P(good), None, None),
+        "ionp_reduce": lambda: L.ionp_reduce(0, P(bad), (ctypes.c_int32 * 1)(0), 1, 0, -1, None, None, P(good), None),
+        "ionp_argext": lambda: L.ionp_argext(1, P(bad), -1, 0, P(good), None),
+        "ionp_accumulate": lambda: L.ionp_accumulate(0, P(bad), 0, P(good), None),
+        "ionp_reduceat": lambda: L.ionp_reduceat(0, P(bad), 0, (ctypes.c_int64 * 1)(0), 1, P(good), None),
+    }
+    for name, fn in calls.items():
+        st = fn()
+        assert st == want, f"{name}: status {st}, want {want}"
+        assert msg in _lib.last_error(), f"{name}: {_lib.last_error()!r}"
+
+
+def test_null_descriptor_and_bad_indices():
+    L = _lib.load_library()
+    good = _arr()
+    assert L.ionp_binary(0, None, ctypes.byref(good), ctypes.byref(good), None, None, None) == _lib.ERR_INVALID
+    assert "is NULL" in _lib.last_error()
+    assert L.ionp_reduceat(0, ctypes.byref(good), 0, None, 3, ctypes.byref(good), None) == _lib.ERR_INVALID
+    assert L.ionp_reduceat(0, ctypes.byref(good), 0, None, -1, ctypes.byref(good), None) == _lib.ERR_INVALID

@@ -321,3 +321,37 @@ def test_axis0_float_add_nan_payloads(shape, dt):
     check_reduce("add", a, d, axis=0)
     check_reduce("add", a, d, axis=0, initial=0.5)
     check_reduce("add", a, d, axis=0, keepdims=True)
+
+
+@pytest.mark.parametrize("shape,axis", [((64, 4096), 1), ((9, 32768), -1), ((3, 1 << 20), 1), ((1 << 22,), None),
+                                        ((2, 16, 8192), (1, 2)), ((5, 65536), None)])
+def test_float32_power_of_two_runs(shape, axis):
+    """float32 add.reduce over power-of-two runs (the bulk-copy window
+    kernel): NaN payloads of both signs, +inf / -inf pairs whose sum is the
+    x86 default NaN, leaves with several NaN chains, split runs."""
+    rng = np.random.default_rng(71)
+    a = rng.standard_normal(shape, dtype=np.float32)
+    flat = a.reshape(-1)
+    n = flat.size
+    pos = rng.permutation(n)
+    k = max(n // 1000, 4)
+    flat[pos[:k]] = np.array([0x7FC01234, 0xFFC05678, 0x7F800001, 0xFFA00000], np.uint32).view(np.float32)[np.arange(k) % 4]
+    flat[pos[k:2 * k]] = np.inf
+    flat[pos[2 * k:3 * k]] = -np.inf
+    flat[pos[3 * k:4 * k]] = -0.0
+    want = np.asarray(O.reduce("add", a, axis=axis))
+    got = ap.add.reduce(ap.from_numpy(a), axis=axis)
+    assert_bits_equal(np.asarray(got.get() if isinstance(got, ap.ndarray) else got).reshape(want.shape), want,
+                      f"float32 add.reduce {shape} axis={axis}")
+    # clean data: no NaN anywhere, the plain-add fast path alone
+    b = rng.standard_normal(shape, dtype=np.float32)
+    want = np.asarray(O.reduce("add", b, axis=axis, keepdims=True))
+    got = ap.add.reduce(ap.from_numpy(b), axis=axis, keepdims=True)
+    assert_bits_equal(got.get(), want, f"float32 add.reduce clean {shape}")
+    # a view whose rows start off a 16-byte boundary takes another kernel
+    if len(shape) == 2 and axis in (1, -1):
+        c = rng.standard_normal((shape[0], shape[1] + 1), dtype=np.float32)
+        v = c[:, 1:]
+        want = np.asarray(O.reduce("add", v, axis=1))
+        got = ap.add.reduce(ap.from_numpy(c)[:, 1:], axis=1)
+        assert_bits_equal(got.get(), want, f"float32 add.reduce misaligned {shape}")
