@@ -112,13 +112,22 @@ int32_t run_row(RedDesc& d, cudaStream_t s) {
         RedDesc t = d;
         t.K = 0;
         if (pw32_ok(t)) {
-            // units of 2^p windows, p as large as keeps >= 8 units per warp
+            // units of 2^p windows spread round-robin over the resident
+            // warps: the smallest split whose units give every warp an
+            // equal share to within 3 % (else the most even one)
             int kw = 0;
             while ((w >> kw) > PW32_WIN) ++kw;
-            const int64_t want_units = (int64_t)sm_count() * 6 * 8;
-            int kk = kw;
-            while (kk > 0 && (d.nout << (kk - 1)) >= want_units) --kk;
-            if (kk <= 2 * TOP_CHUNK_LOG && kk >= K) K = kk;
+            const int64_t gw = pw32_resident_warps();
+            int pick = 0;
+            double best = -1.0;
+            for (int kk = 0; kk <= std::min(kw, 2 * TOP_CHUNK_LOG); ++kk) {
+                const int64_t units = d.nout << kk;
+                const int64_t per = (units + gw - 1) / gw;
+                const double eff = (double)units / ((double)gw * (double)per);
+                if (eff >= 0.97) { pick = kk; break; }
+                if (eff > best + 1e-9) { best = eff; pick = kk; }
+            }
+            K = pick;
         }
     }
     auto lens = seg_lengths(w, K);

@@ -350,6 +350,84 @@ k_bin_trv(EwDesc d, uint32_t* flags) {
     if constexpr (FPE) flush_flags(bits, flags);
 }
 
+// Tile kernel for exactly one operand laid out across the output (the other
+// follows it): only that operand goes through shared memory; the other is
+// read straight into registers at the output's positions; and the next
+// tile's transposed vectors are loaded while this tile is computed, so each
+// thread keeps one tile of loads in flight through the arithmetic.
+template <int OP, int CD, bool FPE>
+__global__ void __launch_bounds__(EW_THREADS)
+k_bin_trv1(EwDesc d, uint32_t* flags) {
+    typedef typename DT<CD>::T T;
+    typedef BinOp<OP, CD> Op;
+    typedef typename Op::R R;
+    typedef TrV<T> V;
+    static_assert(sizeof(R) == sizeof(T), "the vector path stores results of the operand width");
+    __shared__ T st[V::TILE][V::TILE + 1];
+    uint32_t bits = 0;
+    const int64_t tc = d.shape[1] / V::TILE, nt = (d.shape[0] / V::TILE) * tc;
+    const bool ocol = d.so[0] == 1;
+    const bool swap = (d.a.st[0] == 1) == ocol;  // a follows the output: b is the one across
+    const T* pt = (const T*)(swap ? d.b.p : d.a.p);
+    const T* pd = (const T*)(swap ? d.a.p : d.b.p);
+    const int64_t t0 = swap ? d.b.st[0] : d.a.st[0], t1 = swap ? d.b.st[1] : d.a.st[1];
+    const int64_t q0 = swap ? d.a.st[0] : d.b.st[0], q1 = swap ? d.a.st[1] : d.b.st[1];
+    R* po = (R*)d.o;
+    const int tid = threadIdx.x;
+    const int lane_v = (tid % V::TPR) * V::VW, line = tid / V::TPR;
+    constexpr int LSTEP = EW_THREADS / V::TPR;
+    Vec16<T> rt[V::PASS];
+    auto fetch = [&](int64_t t) {
+        const int64_t i0 = (t / tc) * V::TILE, j0 = (t % tc) * V::TILE;
+#pragma unroll
+        for (int k = 0; k < V::PASS; ++k) {
+            const int w = line + k * LSTEP;
+            rt[k] = (t0 == 1) ? ldv(pt + (i0 + lane_v) + (j0 + w) * t1, 0) : ldv(pt + (i0 + w) * t0 + (j0 + lane_v), 0);
+        }
+    };
+    int64_t t = blockIdx.x;
+    if (t < nt) fetch(t);
+    for (; t < nt; t += gridDim.x) {
+#pragma unroll
+        for (int k = 0; k < V::PASS; ++k) {
+            const int w = line + k * LSTEP;
+            if (t0 == 1) {
+#pragma unroll
+                for (int e = 0; e < V::VW; ++e) st[lane_v + e][w] = rt[k].v[e];
+            } else {
+#pragma unroll
+                for (int e = 0; e < V::VW; ++e) st[w][lane_v + e] = rt[k].v[e];
+            }
+        }
+        __syncthreads();
+        const int64_t i0 = (t / tc) * V::TILE, j0 = (t % tc) * V::TILE;
+        Vec16<T> xd[V::PASS];
+#pragma unroll
+        for (int k = 0; k < V::PASS; ++k) {
+            const int m = line + k * LSTEP;
+            xd[k] = ocol ? ldv(pd + (i0 + lane_v) + (j0 + m) * q1, 0) : ldv(pd + (i0 + m) * q0 + (j0 + lane_v), 0);
+        }
+        if (t + gridDim.x < nt) fetch(t + gridDim.x);
+#pragma unroll
+        for (int k = 0; k < V::PASS; ++k) {
+            const int m = line + k * LSTEP;
+            R r[V::VW];
+#pragma unroll
+            for (int e = 0; e < V::VW; ++e) {
+                const T vt = ocol ? st[lane_v + e][m] : st[m][lane_v + e];
+                const T vd = xd[k].v[e];
+                const T x = swap ? vd : vt, y = swap ? vt : vd;
+                r[e] = Op::apply(x, y);
+                if constexpr (FPE) bits |= fpe_bits<OP, CD>(x, y, r[e]);
+            }
+            R* dst = ocol ? po + (i0 + lane_v) + (j0 + m) * d.so[1] : po + (i0 + m) * d.so[0] + (j0 + lane_v);
+            stv<R, V::VW>(dst, 0, r);
+        }
+        __syncthreads();
+    }
+    if constexpr (FPE) flush_flags(bits, flags);
+}
+
 // ---------------------------------------------------------------------------
 // unary
 // ---------------------------------------------------------------------------

@@ -65,6 +65,17 @@ cudaError_t launch_bin_t(const EwDesc& d, const ContigInfo& ci, uint32_t* flags,
                 if (trv_ok<T>(d)) {
                     constexpr int TL = TrV<T>::TILE;
                     const int64_t tiles = (d.shape[0] / TL) * (d.shape[1] / TL);
+                    if constexpr (sizeof(T) == 4) {
+                        if ((ca != co) != (cb != co)) {  // one operand across the output
+                            const int g = (int)(tiles < sm_count() * 8 ? tiles : sm_count() * 8);
+                            if constexpr (HAS_FPE) {
+                                if (fpe) { k_bin_trv1<OP, CD, true><<<g, EW_THREADS, 0, s>>>(d, flags); count_launch(); return cudaGetLastError(); }
+                            }
+                            k_bin_trv1<OP, CD, false><<<g, EW_THREADS, 0, s>>>(d, flags);
+                            count_launch();
+                            return cudaGetLastError();
+                        }
+                    }
                     const int g = (int)(tiles < sm_count() * 6 ? tiles : sm_count() * 6);
                     if constexpr (HAS_FPE) {
                         if (fpe) { k_bin_trv<OP, CD, true><<<g, EW_THREADS, 0, s>>>(d, flags); count_launch(); return cudaGetLastError(); }

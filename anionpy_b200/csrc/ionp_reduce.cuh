@@ -562,6 +562,76 @@ __global__ void __launch_bounds__(RED_THREADS) k_red_col(RedDesc d) {
     }
 }
 
+// One batch of a column fold in order: float add sums plainly and replays
+// the batch with the engine's NaN rule only when the sum turns NaN (once the
+// accumulator is a quiet NaN no later add changes it).
+template <int OP, int CD, int U>
+__device__ __forceinline__ void col_fold_batch(typename DT<CD>::T& acc, const typename DT<CD>::T (&x)[U]) {
+    typedef typename DT<CD>::T T;
+    if constexpr (OP == OP_ADD && (CD == DT_F32 || CD == DT_F64)) {
+        if (acc == acc) {
+            T r = acc;
+#pragma unroll
+            for (int u = 0; u < U; ++u) r = plain_sum(r, x[u]);
+            if (r != r) {
+                r = acc;
+#pragma unroll
+                for (int u = 0; u < U; ++u) r = BinOp<OP, CD>::apply(r, x[u]);
+            }
+            acc = r;
+        } else {
+            acc = BinOp<OP, CD>::apply(acc, x[0]);  // quiets a signaling NaN once
+        }
+    } else {
+#pragma unroll
+        for (int u = 0; u < U; ++u) acc = BinOp<OP, CD>::apply(acc, x[u]);
+    }
+}
+
+// COL kernel, pipelined: one narrow axis, input in the loop dtype, too few
+// outputs for one batch of loads per thread to keep HBM busy. One thread per
+// output folds its column in order; its loads come in batches of U held in
+// two register buffers, the next batch issued before the current one is
+// folded, so U to 2U loads stay in flight per thread through the fold.
+constexpr int COLP_THREADS = 128;
+template <int OP, int CD, int U>
+__global__ void __launch_bounds__(COLP_THREADS) k_red_col_pipe(RedDesc d) {
+    typedef typename DT<CD>::T T;
+    const int64_t n = d.rshape[0], rs = d.rst[0];
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t o = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; o < d.nout; o += stride) {
+        int64_t base, out_off;
+        kept_offsets(d, o, &base, &out_off);
+        const T* p = reinterpret_cast<const T*>(d.a) + base;
+        T acc;
+        memcpy(&acc, &d.seed, sizeof(T));
+        int64_t j = 0;
+        if (!d.has_seed && n > 0) { acc = p[0]; j = 1; }
+        const int64_t nb = (n - j) / U;
+        T xa[U], xb[U];
+        if (nb > 0) {
+#pragma unroll
+            for (int u = 0; u < U; ++u) xa[u] = p[(j + u) * rs];
+            int64_t b = 0;
+            for (; b + 2 <= nb; b += 2) {
+                const T* q = p + (j + (b + 1) * U) * rs;
+#pragma unroll
+                for (int u = 0; u < U; ++u) xb[u] = q[u * rs];
+                col_fold_batch<OP, CD, U>(acc, xa);
+                if (b + 2 < nb) {
+                    const T* q2 = q + U * rs;
+#pragma unroll
+                    for (int u = 0; u < U; ++u) xa[u] = q2[u * rs];
+                }
+                col_fold_batch<OP, CD, U>(acc, xb);
+            }
+            if (b < nb) col_fold_batch<OP, CD, U>(acc, xa);
+        }
+        for (int64_t i = j + nb * U; i < n; ++i) acc = BinOp<OP, CD>::apply(acc, p[i * rs]);
+        store_cast<CD>(d.o, out_off, d.odt, acc);
+    }
+}
+
 // COL kernel, split: one narrow axis folded by an order-free (associative)
 // op. Too few outputs to keep HBM busy with one thread each, so the axis is
 // cut into 2^K contiguous parts; task t folds part t / nout of output

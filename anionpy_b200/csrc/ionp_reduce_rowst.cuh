@@ -698,22 +698,25 @@ __global__ void __launch_bounds__(RED_THREADS, NAR_CTAS) k_red_rownar(RedDesc d)
 // ---------------------------------------------------------------------------
 // Host side: which rows take these kernels, and their launch.
 // ---------------------------------------------------------------------------
-// ---------------------------------------------------------------------------
 // k_red_pw32: float32 add over runs of 2^m >= 4096 elements, the common
 // case of a row or whole-array sum. For such runs numpy's pairwise tree
 // (ufunc.rs:6416-6448) halves exactly down to 128-element leaves, so the
 // run is a perfect tree of 4096-element windows, each a perfect tree of 32
 // leaves. One warp takes one window at a time:
-//  * load: every lane issues one 512-byte bulk copy (cp.async.bulk, the TMA
-//    engine, unicast from this GPU's memory) of its leaf into a padded
-//    shared slot, completing on the stage's mbarrier; two stages per warp;
+//  * load: G lanes each issue one bulk copy (cp.async.bulk, the TMA engine,
+//    unicast from this GPU's memory) of 32 / G consecutive leaves into a
+//    shared group slot padded by 16 bytes, completing on the stage's
+//    mbarrier; two stages per warp. Lane l takes leaf (l % G) * (32 / G) +
+//    l / G, so the 8 lanes of each 16-byte shared-load phase read 8
+//    different groups, on different banks (G = 8: four times fewer copies
+//    than one per leaf, which measured 15 % faster);
 //  * leaf: the lane sums its 128 elements as 8 independent chains of plain
 //    adds (elements k, k+8, ...), combined ((r0+r1)+(r2+r3))+((r4+r5)+
 //    (r6+r7)). A chain that comes out NaN is summed again with the engine's
 //    add (the x86 NaN rules) and the combine redone with it: a result that
 //    is not NaN had no NaN in it, so plain adds give the same bits;
-//  * window: the 32 leaf sums fold across lanes by shuffles, left operand
-//    first (a perfect tree);
+//  * window: the 32 leaf sums fold across lanes by shuffles from the lane
+//    holding the partner leaf, left operand first (a perfect tree);
 //  * run: window sums fold on a binary-counter stack (push; while the two
 //    top entries have the same height, fold them), which rebuilds the
 //    perfect tree over a unit's 2^p windows.
@@ -721,13 +724,13 @@ __global__ void __launch_bounds__(RED_THREADS, NAR_CTAS) k_red_rownar(RedDesc d)
 // d.err, drains the warp's copies (again with a limit) and ends the warp.
 // ---------------------------------------------------------------------------
 constexpr int PW32_WIN = 4096;
-constexpr int PW32_PITCH = 132;      // floats per shared leaf slot (16 bytes of padding)
-constexpr int PW32_STAGES = 2;
-constexpr int PW32_WARPS = 2;
 constexpr int PW32_STACK = 24;
-constexpr size_t PW32_STAGE_BYTES = (size_t)32 * PW32_PITCH * sizeof(float);
-constexpr size_t PW32_WARP_SMEM = PW32_STAGES * PW32_STAGE_BYTES + 64 + PW32_STACK * 8;
-constexpr size_t PW32_SMEM = PW32_WARPS * PW32_WARP_SMEM;
+// ST stages per warp, NW warps per CTA
+// G bulk copies per window, each of 32 / G leaves; a group's shared slot is
+// padded by 16 bytes
+template <int G> constexpr size_t pw32_stage_bytes() { return (size_t)G * ((32 / G) * 512 + 16); }
+template <int ST, int G> constexpr size_t pw32_warp_smem() { return ST * pw32_stage_bytes<G>() + 64 + PW32_STACK * 8; }
+template <int ST, int NW, int G> constexpr size_t pw32_smem() { return NW * pw32_warp_smem<ST, G>(); }
 constexpr long long PW32_SPIN_LIMIT = 1LL << 26;
 
 __device__ __forceinline__ void mbar_init(uint64_t* bar, unsigned count) {
@@ -759,15 +762,17 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned by
                  ::"r"(d), "l"(src), "r"(bytes), "r"(b) : "memory");
 }
 
-template <int OP, int CD>
+template <int OP, int CD, int PW32_STAGES, int PW32_WARPS, int G>
 __global__ void __launch_bounds__(32 * PW32_WARPS) k_red_pw32(RedDesc d) {
+    constexpr int LPG = 32 / G;                          // leaves per copy
+    constexpr int GP = LPG * 128 + 4;                    // floats per group slot
     typedef RPol<OP, CD> P;
     static_assert(CD == DT_F32 && OP == OP_ADD, "float32 add only");
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    unsigned char* wb = smem_raw + (size_t)warp * PW32_WARP_SMEM;
+    unsigned char* wb = smem_raw + (size_t)warp * pw32_warp_smem<PW32_STAGES, G>();
     float* ring = reinterpret_cast<float*>(wb);
-    uint64_t* bar = reinterpret_cast<uint64_t*>(wb + PW32_STAGES * PW32_STAGE_BYTES);
+    uint64_t* bar = reinterpret_cast<uint64_t*>(wb + PW32_STAGES * pw32_stage_bytes<G>());
     float* stk = reinterpret_cast<float*>(bar + 8);
     int* stk_h = reinterpret_cast<int*>(stk + PW32_STACK);
     const int64_t nseg = (int64_t)1 << d.K;
@@ -797,7 +802,7 @@ __global__ void __launch_bounds__(32 * PW32_WARPS) k_red_pw32(RedDesc d) {
         const int s = (int)(iq % PW32_STAGES);
         if (lane == 0) mbar_expect_tx(&bar[s], 32 * 512);
         __syncwarp();
-        bulk_g2s(ring + (size_t)s * 32 * PW32_PITCH + lane * PW32_PITCH, ibase + ij * PW32_WIN + lane * 128, 512, &bar[s]);
+        if (lane < G) bulk_g2s(ring + (size_t)s * G * GP + lane * GP, ibase + ij * PW32_WIN + lane * LPG * 128, LPG * 512, &bar[s]);
         ++iq;
         if (++ij == wpu) {
             ij = 0;
@@ -814,10 +819,14 @@ __global__ void __launch_bounds__(32 * PW32_WARPS) k_red_pw32(RedDesc d) {
             if (!mbar_wait_bounded(&bar[s], (unsigned)((q / PW32_STAGES) & 1))) {
                 // give up: record it, drain this warp's other copy, end the warp
                 if (lane == 0 && d.err) atomicOr(d.err, 1u);
-                if (iq > q + 1) mbar_wait_bounded(&bar[(q + 1) % PW32_STAGES], (unsigned)(((q + 1) / PW32_STAGES) & 1));
+                for (int64_t q2 = q + 1; q2 < iq; ++q2)
+                    if (!mbar_wait_bounded(&bar[q2 % PW32_STAGES], (unsigned)((q2 / PW32_STAGES) & 1))) break;
                 return;
             }
-            const float* lp = ring + (size_t)s * 32 * PW32_PITCH + lane * PW32_PITCH;
+            // lane l holds leaf (l % G) * LPG + l / G: the 8 lanes of each
+            // 16-byte shared load phase read 8 different groups, whose
+            // 16-byte pads put them on different banks
+            const float* lp = ring + (size_t)s * G * GP + (lane % G) * GP + (lane / G) * 128;
             float r[8];
 #pragma unroll
             for (int jj = 0; jj < 16; ++jj) {
@@ -848,10 +857,12 @@ __global__ void __launch_bounds__(32 * PW32_WARPS) k_red_pw32(RedDesc d) {
             }
             __syncwarp();  // every lane has read this stage before it is refilled
             float v = leaf;
+            const int L = (lane % G) * LPG + lane / G;  // this lane's leaf
 #pragma unroll
             for (int h = 1; h < 32; h <<= 1) {
-                const float o = __shfl_down_sync(0xffffffffu, v, h);
-                if ((lane & (2 * h - 1)) == 0) v = P::fold(v, o);
+                const int M = (L + h) & 31;                 // partner leaf (unused past 31)
+                const float o = __shfl_sync(0xffffffffu, v, (M % LPG) * G + M / LPG);
+                if ((L & (2 * h - 1)) == 0) v = P::fold(v, o);
             }
             if (lane == 0) {
                 if (wpu == 1) {
@@ -881,6 +892,42 @@ __global__ void __launch_bounds__(32 * PW32_WARPS) k_red_pw32(RedDesc d) {
             }
         }
     }
+}
+
+template <int ST, int NW, int G> inline int pw32_ctas_per_sm() {
+    static int per_sm = 0;
+    if (per_sm == 0) {
+        auto k = k_red_pw32<OP_ADD, DT_F32, ST, NW, G>;
+        int n = 0;
+        if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pw32_smem<ST, NW, G>()) != cudaSuccess ||
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k, 32 * NW, pw32_smem<ST, NW, G>()) != cudaSuccess || n <= 0) {
+            cudaGetLastError();
+            n = 1;
+        }
+        per_sm = n;
+    }
+    return per_sm;
+}
+
+// the configuration k_red_pw32 runs in: two stages per warp, two warps per
+// CTA, eight bulk copies (of four leaves each) per window
+constexpr int PW32_ST = 2, PW32_NW = 2, PW32_G = 8;
+
+// warps of the float32 window kernel resident on the current device
+inline int64_t pw32_resident_warps() {
+    return (int64_t)sm_count() * pw32_ctas_per_sm<PW32_ST, PW32_NW, PW32_G>() * PW32_NW;
+}
+
+template <int OP, int CD, int ST, int NW, int G>
+static cudaError_t launch_pw32(const RedDesc& din, cudaStream_t s) {
+    auto k = k_red_pw32<OP, CD, ST, NW, G>;
+    const int per_sm = pw32_ctas_per_sm<ST, NW, G>();
+    const int64_t units = din.nout << din.K;
+    const int64_t ctas = (units + NW - 1) / NW;
+    const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(ctas, (int64_t)sm_count() * per_sm));
+    k<<<grid, 32 * NW, pw32_smem<ST, NW, G>(), s>>>(din);
+    count_launch();
+    return cudaGetLastError();
 }
 
 // Runs k_red_pw32 handles: float32 add, input contiguous along the run in
@@ -989,17 +1036,7 @@ static cudaError_t launch_row_wide(const RedDesc& din, cudaStream_t s) {
     }
     if constexpr (OP == OP_ADD && CD == DT_F32) {
         if (pw32_ok(din)) {
-            auto k = k_red_pw32<OP, CD>;
-            cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)PW32_SMEM);
-            if (e != cudaSuccess) return e;
-            int per_sm = 1;
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, 32 * PW32_WARPS, PW32_SMEM);
-            const int64_t units = din.nout << din.K;
-            const int64_t ctas = (units + PW32_WARPS - 1) / PW32_WARPS;
-            const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(ctas, (int64_t)sm_count() * std::max(per_sm, 1)));
-            k<<<grid, 32 * PW32_WARPS, PW32_SMEM, s>>>(din);
-            count_launch();
-            return cudaGetLastError();
+            return launch_pw32<OP, CD, PW32_ST, PW32_NW, PW32_G>(din, s);
         }
     }
     if constexpr (rowst_type_ok(OP, CD)) {

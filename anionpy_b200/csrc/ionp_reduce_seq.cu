@@ -41,12 +41,13 @@ static cudaError_t col_op(const RedDesc& d, cudaStream_t s) {
     const bool castld = d.adt != d.cd;
     const int grid = seq_grid(d.nout, RED_THREADS);
     // fewer than 64K outputs over one long narrow axis of 4- or 8-byte
-    // elements: one thread per output with 64 loads in flight
+    // elements: one thread per output, two register batches of loads
     if (!castld && d.nr == 1 && d.nout < 65536 && d.rshape[0] >= 256 && dt_size(d.cd) >= 4) {
+        const int pgrid = seq_grid(d.nout, COLP_THREADS);
 #define IONP_U64CASE(D)                                                                  \
         case D:                                                                          \
             if constexpr (red_any_valid(OPV, D) && (sizeof(typename DT<D>::T) >= 4)) {   \
-                k_red_col<OPV, D, false, 64><<<grid, RED_THREADS, 0, s>>>(d);            \
+                k_red_col_pipe<OPV, D, 32><<<pgrid, COLP_THREADS, 0, s>>>(d);            \
                 count_launch();                                                          \
                 return cudaGetLastError();                                               \
             }                                                                            \
