@@ -352,8 +352,8 @@ k_bin_trv(EwDesc d, uint32_t* flags) {
 
 // Tile kernel for exactly one operand laid out across the output (the other
 // follows it): only that operand goes through shared memory; the other is
-// read straight into registers at the output's positions; and the next
-// tile's transposed vectors are loaded while this tile is computed, so each
+// read straight into registers at the output's positions; and both
+// operands of the next tile are loaded while this tile is computed, so each
 // thread keeps one tile of loads in flight through the arithmetic.
 template <int OP, int CD, bool FPE>
 __global__ void __launch_bounds__(EW_THREADS)
@@ -376,21 +376,25 @@ k_bin_trv1(EwDesc d, uint32_t* flags) {
     const int tid = threadIdx.x;
     const int lane_v = (tid % V::TPR) * V::VW, line = tid / V::TPR;
     constexpr int LSTEP = EW_THREADS / V::TPR;
-    Vec16<T> rt[V::PASS];
+    // both operands of the next tile are loaded while this one is computed
+    Vec16<T> rt[V::PASS], xn[V::PASS];
     auto fetch = [&](int64_t t) {
         const int64_t i0 = (t / tc) * V::TILE, j0 = (t % tc) * V::TILE;
 #pragma unroll
         for (int k = 0; k < V::PASS; ++k) {
             const int w = line + k * LSTEP;
             rt[k] = (t0 == 1) ? ldv(pt + (i0 + lane_v) + (j0 + w) * t1, 0) : ldv(pt + (i0 + w) * t0 + (j0 + lane_v), 0);
+            xn[k] = ocol ? ldv(pd + (i0 + lane_v) + (j0 + w) * q1, 0) : ldv(pd + (i0 + w) * q0 + (j0 + lane_v), 0);
         }
     };
     int64_t t = blockIdx.x;
     if (t < nt) fetch(t);
     for (; t < nt; t += gridDim.x) {
+        Vec16<T> xd[V::PASS];
 #pragma unroll
         for (int k = 0; k < V::PASS; ++k) {
             const int w = line + k * LSTEP;
+            xd[k] = xn[k];
             if (t0 == 1) {
 #pragma unroll
                 for (int e = 0; e < V::VW; ++e) st[lane_v + e][w] = rt[k].v[e];
@@ -401,12 +405,6 @@ k_bin_trv1(EwDesc d, uint32_t* flags) {
         }
         __syncthreads();
         const int64_t i0 = (t / tc) * V::TILE, j0 = (t % tc) * V::TILE;
-        Vec16<T> xd[V::PASS];
-#pragma unroll
-        for (int k = 0; k < V::PASS; ++k) {
-            const int m = line + k * LSTEP;
-            xd[k] = ocol ? ldv(pd + (i0 + lane_v) + (j0 + m) * q1, 0) : ldv(pd + (i0 + m) * q0 + (j0 + lane_v), 0);
-        }
         if (t + gridDim.x < nt) fetch(t + gridDim.x);
 #pragma unroll
         for (int k = 0; k < V::PASS; ++k) {

@@ -65,8 +65,12 @@ cudaError_t launch_bin_t(const EwDesc& d, const ContigInfo& ci, uint32_t* flags,
                 if (trv_ok<T>(d)) {
                     constexpr int TL = TrV<T>::TILE;
                     const int64_t tiles = (d.shape[0] / TL) * (d.shape[1] / TL);
-                    if constexpr (sizeof(T) == 4) {
-                        if ((ca != co) != (cb != co)) {  // one operand across the output
+                    // one operand across the output: 4-byte types, and the
+                    // division family of 8-byte types (arithmetic-heavy,
+                    // where overlapping the next tile's loads pays)
+                    constexpr bool DIVF = OP == OP_FLOOR_DIVIDE || OP == OP_REMAINDER || OP == OP_FMOD || OP == OP_DIVIDE;
+                    if constexpr (sizeof(T) == 4 || DIVF) {
+                        if ((ca != co) != (cb != co)) {
                             const int g = (int)(tiles < sm_count() * 8 ? tiles : sm_count() * 8);
                             if constexpr (HAS_FPE) {
                                 if (fpe) { k_bin_trv1<OP, CD, true><<<g, EW_THREADS, 0, s>>>(d, flags); count_launch(); return cudaGetLastError(); }

@@ -154,6 +154,11 @@ __host__ __device__ __forceinline__ int64_t pw_split(int64_t len) {
 
 // Offsets of output index `o` over the kept dims: input and output.
 __device__ __forceinline__ void kept_offsets(const RedDesc& d, int64_t o, int64_t* in_off, int64_t* out_off) {
+    if (d.nk == 1) {  // o < kshape[0]: no division
+        *in_off = o * d.kst[0];
+        *out_off = o * d.kost[0];
+        return;
+    }
     int64_t a = 0, b = 0;
     for (int k = d.nk - 1; k >= 0; --k) {
         int64_t s = d.kshape[k];
@@ -651,16 +656,35 @@ __global__ void __launch_bounds__(RED_THREADS) k_red_col_split(RedDesc d) {
         const int64_t r0 = part * len / P, r1 = (part + 1) * len / P;
         const T* p = (const T*)d.a + base;
         T acc = p[r0 * rs];
-        int64_t j = r0 + 1;
+        const int64_t j = r0 + 1;
+        // batches of 16 loads in two register buffers, the next issued
+        // before the current one is folded
         constexpr int U = 16;
-        for (; j + U <= r1; j += U) {
-            T x[U];
+        const int64_t nb = (r1 - j) / U;
+        T xa[U], xb[U];
+        if (nb > 0) {
 #pragma unroll
-            for (int u = 0; u < U; ++u) x[u] = p[(j + u) * rs];
+            for (int u = 0; u < U; ++u) xa[u] = p[(j + u) * rs];
+            int64_t b = 0;
+            for (; b + 2 <= nb; b += 2) {
+                const T* q = p + (j + (b + 1) * U) * rs;
 #pragma unroll
-            for (int u = 0; u < U; ++u) acc = BinOp<OP, CD>::apply(acc, x[u]);
+                for (int u = 0; u < U; ++u) xb[u] = q[u * rs];
+#pragma unroll
+                for (int u = 0; u < U; ++u) acc = BinOp<OP, CD>::apply(acc, xa[u]);
+                if (b + 2 < nb) {
+#pragma unroll
+                    for (int u = 0; u < U; ++u) xa[u] = q[(U + u) * rs];
+                }
+#pragma unroll
+                for (int u = 0; u < U; ++u) acc = BinOp<OP, CD>::apply(acc, xb[u]);
+            }
+            if (b < nb) {
+#pragma unroll
+                for (int u = 0; u < U; ++u) acc = BinOp<OP, CD>::apply(acc, xa[u]);
+            }
         }
-        for (; j < r1; ++j) acc = BinOp<OP, CD>::apply(acc, p[j * rs]);
+        for (int64_t k = j + nb * U; k < r1; ++k) acc = BinOp<OP, CD>::apply(acc, p[k * rs]);
         reinterpret_cast<T*>(d.scratch)[o * P + part] = acc;
     }
 }
@@ -1250,10 +1274,37 @@ __global__ void __launch_bounds__(RED_THREADS) k_argext_top(RedDesc d) {
 // with d.K > 0 the axis is cut into 2^K contiguous parts (task t scans part
 // t / nout of output t % nout) whose (value, index) partials k_argext_top
 // combines.
+// One batch of an in-order argmin/argmax scan: `best`/`bi` updated from
+// x[0..U) at indices i0..i0+U. Without a NaN on either side "better" is a
+// strict comparison (float16 compares through float in P::better).
+template <int CD, bool MAX, int U>
+__device__ __forceinline__ void argext_batch(typename DT<CD>::T& best, int64_t& bi, const typename DT<CD>::T (&x)[U],
+                                             int64_t i0) {
+    typedef ArgPol<CD, MAX> P;
+    bool nan = false;
+    if constexpr (dt_is_float(CD)) {
+#pragma unroll
+        for (int u = 0; u < U; ++u) nan |= P::is_nan(x[u]);
+        nan |= P::is_nan(best);
+    }
+    if (CD != DT_F16 && !nan) {
+#pragma unroll
+        for (int u = 0; u < U; ++u)
+            if (MAX ? (x[u] > best) : (x[u] < best)) { best = x[u]; bi = i0 + u; }
+    } else {
+#pragma unroll
+        for (int u = 0; u < U; ++u) if (P::better(x[u], best)) { best = x[u]; bi = i0 + u; }
+    }
+}
+
+// Column scan: task t = (part, output) scans rows [r0, r1) of its output's
+// column in order, loads in batches of 16 held in two register buffers (the
+// next batch issued before the current one is scanned).
 template <int CD, bool MAX>
 __global__ void __launch_bounds__(RED_THREADS) k_argext_col(RedDesc d) {
     typedef ArgPol<CD, MAX> P;
     typedef typename DT<CD>::T T;
+    constexpr int U = 16;
     const int64_t nseg = (int64_t)1 << d.K;
     const int64_t ntask = d.nout * nseg;
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
@@ -1265,32 +1316,29 @@ __global__ void __launch_bounds__(RED_THREADS) k_argext_col(RedDesc d) {
         const T* p = (const T*)d.a + base;
         T best = p[r0 * d.ws];
         int64_t bi = r0;
-        int64_t i = r0 + 1;
-        constexpr int U = 16;
-        for (; i + U <= r1; i += U) {
-            T x[U];
+        const int64_t i = r0 + 1;
+        const int64_t nb = (r1 - i) / U;
+        T xa[U], xb[U];
+        if (nb > 0) {
 #pragma unroll
-            for (int u = 0; u < U; ++u) x[u] = p[(i + u) * d.ws];
-            bool nan = false;
-            if constexpr (dt_is_float(CD)) {
+            for (int u = 0; u < U; ++u) xa[u] = p[(i + u) * d.ws];
+            int64_t b = 0;
+            for (; b + 2 <= nb; b += 2) {
+                const int64_t i1 = i + (b + 1) * U;
 #pragma unroll
-                for (int u = 0; u < U; ++u) nan |= P::is_nan(x[u]);
-                nan |= P::is_nan(best);
+                for (int u = 0; u < U; ++u) xb[u] = p[(i1 + u) * d.ws];
+                argext_batch<CD, MAX, U>(best, bi, xa, i1 - U);
+                if (b + 2 < nb) {
+#pragma unroll
+                    for (int u = 0; u < U; ++u) xa[u] = p[(i1 + U + u) * d.ws];
+                }
+                argext_batch<CD, MAX, U>(best, bi, xb, i1);
             }
-            if (CD != DT_F16 && !nan) {
-                // no NaN on either side: "better" is a strict comparison
-                // (float16 compares through float in P::better)
-#pragma unroll
-                for (int u = 0; u < U; ++u)
-                    if (MAX ? (x[u] > best) : (x[u] < best)) { best = x[u]; bi = i + u; }
-            } else {
-#pragma unroll
-                for (int u = 0; u < U; ++u) if (P::better(x[u], best)) { best = x[u]; bi = i + u; }
-            }
+            if (b < nb) argext_batch<CD, MAX, U>(best, bi, xa, i + b * U);
         }
-        for (; i < r1; ++i) {
-            T x = p[i * d.ws];
-            if (P::better(x, best)) { best = x; bi = i; }
+        for (int64_t k = i + nb * U; k < r1; ++k) {
+            T x = p[k * d.ws];
+            if (P::better(x, best)) { best = x; bi = k; }
         }
         if (d.K == 0) {
             ((int64_t*)d.o)[out_off] = bi;

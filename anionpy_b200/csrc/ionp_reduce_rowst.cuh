@@ -762,6 +762,9 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned by
                  ::"r"(d), "l"(src), "r"(bytes), "r"(b) : "memory");
 }
 
+// the lane holding leaf L when G bulk copies of 32 / G leaves fill a window
+template <int G> __host__ __device__ constexpr int pw32_leaf_lane(int L) { return (L % (32 / G)) * G + L / (32 / G); }
+
 template <int OP, int CD, int PW32_STAGES, int PW32_WARPS, int G>
 __global__ void __launch_bounds__(32 * PW32_WARPS) k_red_pw32(RedDesc d) {
     constexpr int LPG = 32 / G;                          // leaves per copy
@@ -856,13 +859,24 @@ __global__ void __launch_bounds__(32 * PW32_WARPS) k_red_pw32(RedDesc d) {
                                P::fold(P::fold(r[4], r[5]), P::fold(r[6], r[7])));
             }
             __syncwarp();  // every lane has read this stage before it is refilled
+            // Leaf sums fold as a butterfly of plain adds: leaf bit t is lane
+            // bit pw32_leaf_lane<G>(1 << t), and the lanes whose lower leaf
+            // bits are clear hold the left-first subtree sums (IEEE addition
+            // is commutative for non-NaN operands). Lane 0 ends with the
+            // window sum; if it is NaN the tree is redone with the engine's
+            // add from the kept leaf sums.
             float v = leaf;
-            const int L = (lane % G) * LPG + lane / G;  // this lane's leaf
 #pragma unroll
-            for (int h = 1; h < 32; h <<= 1) {
-                const int M = (L + h) & 31;                 // partner leaf (unused past 31)
-                const float o = __shfl_sync(0xffffffffu, v, (M % LPG) * G + M / LPG);
-                if ((L & (2 * h - 1)) == 0) v = P::fold(v, o);
+            for (int t = 0; t < 5; ++t) v = __fadd_rn(v, __shfl_xor_sync(0xffffffffu, v, pw32_leaf_lane<G>(1 << t)));
+            if (__shfl_sync(0xffffffffu, v, 0) != __shfl_sync(0xffffffffu, v, 0)) {
+                const int L = (lane % G) * LPG + lane / G;  // this lane's leaf
+                v = leaf;
+#pragma unroll
+                for (int h = 1; h < 32; h <<= 1) {
+                    const int M = (L + h) & 31;             // partner leaf (unused past 31)
+                    const float o = __shfl_sync(0xffffffffu, v, pw32_leaf_lane<G>(M));
+                    if ((L & (2 * h - 1)) == 0) v = P::fold(v, o);
+                }
             }
             if (lane == 0) {
                 if (wpu == 1) {

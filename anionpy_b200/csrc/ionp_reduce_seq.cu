@@ -47,7 +47,7 @@ static cudaError_t col_op(const RedDesc& d, cudaStream_t s) {
 #define IONP_U64CASE(D)                                                                  \
         case D:                                                                          \
             if constexpr (red_any_valid(OPV, D) && (sizeof(typename DT<D>::T) >= 4)) {   \
-                k_red_col_pipe<OPV, D, 32><<<pgrid, COLP_THREADS, 0, s>>>(d);            \
+                k_red_col_pipe<OPV, D, sizeof(typename DT<D>::T) == 4 ? 64 : 32><<<pgrid, COLP_THREADS, 0, s>>>(d); \
                 count_launch();                                                          \
                 return cudaGetLastError();                                               \
             }                                                                            \

@@ -111,18 +111,9 @@ __device__ __forceinline__ double x_sqrt(double x) { return isnan_d(x) ? quiet_d
 // x's sign repairs the one-too-large case exactly. Larger quotients take the
 // library's fmod.
 // the special values and the huge-quotient case, out of line
-static __device__ __noinline__ float x_fmod_full(float x, float y) {
-    if (isnan_f(x) || isnan_f(y)) return nan2(x, y);
-    if (isinf(x) || y == 0.0f) return dnan_f();
-    if (isinf(y)) return x;
-    return fmodf(x, y);
-}
-static __device__ __noinline__ double x_fmod_full(double x, double y) {
-    if (isnan_d(x) || isnan_d(y)) return nan2(x, y);
-    if (isinf(x) || y == 0.0) return dnan_d();
-    if (isinf(y)) return x;
-    return fmod(x, y);
-}
+// quotients of 2^23 (2^52) and more, out of line
+static __device__ __noinline__ float x_fmod_big(float x, float y) { return fmodf(x, y); }
+static __device__ __noinline__ double x_fmod_big(double x, double y) { return fmod(x, y); }
 __device__ __forceinline__ float x_fmod(float x, float y) {
     if (isfinite(x) && isfinite(y) && y != 0.0f) {
         const float q = truncf(__fdiv_rn(x, y));
@@ -131,8 +122,12 @@ __device__ __forceinline__ float x_fmod(float x, float y) {
             if (r != 0.0f && signbit(r) != signbit(x)) r = __fadd_rn(r, copysignf(y, x));
             return r == 0.0f ? copysignf(0.0f, x) : r;
         }
+        return x_fmod_big(x, y);
     }
-    return x_fmod_full(x, y);
+    // the special values, inline (a call here costs every warp that meets one)
+    if (isnan_f(x) || isnan_f(y)) return nan2(x, y);
+    if (isinf(x) || y == 0.0f) return dnan_f();
+    return x;  // y infinite, x finite
 }
 __device__ __forceinline__ double x_fmod(double x, double y) {
     if (isfinite(x) && isfinite(y) && y != 0.0) {
@@ -142,8 +137,11 @@ __device__ __forceinline__ double x_fmod(double x, double y) {
             if (r != 0.0 && signbit(r) != signbit(x)) r = __dadd_rn(r, copysign(y, x));
             return r == 0.0 ? copysign(0.0, x) : r;
         }
+        return x_fmod_big(x, y);
     }
-    return x_fmod_full(x, y);
+    if (isnan_d(x) || isnan_d(y)) return nan2(x, y);
+    if (isinf(x) || y == 0.0) return dnan_d();
+    return x;
 }
 
 // ---------------------------------------------------------------------------
@@ -410,19 +408,50 @@ template <int D> static __device__ __noinline__ typename FOps<D>::T floor_divide
     }
     return O::floor_(O::div(x, y));
 }
+// trunc(x / y) or one more in magnitude, from an approximate quotient, for
+// x finite and 2^-125 <= |y| <= 2^125; false when |x / y| is too large.
+// float32: __fdividef is within 2 ulps here; scaled up by 2^-20 the quotient
+// is at least |x / y| and, below 2^19, less than q + 2 (q = trunc|x / y|).
+// float64: a float32 reciprocal approximation refined by one Newton step is
+// within a relative 2^-42; scaled up by 2^-38 the same holds below 2^36.
+// Either way t is q or q + 1 in magnitude, which the caller's repair step
+// (exact x - t*y, one correction) turns into q exactly.
+__device__ __forceinline__ bool trunc_quot_approx(float x, float y, float* t) {
+    const float ay = fabsf(y);
+    if (!(ay >= 0x1p-125f && ay <= 0x1p125f)) return false;
+    const float pu = __fmul_rn(__fdividef(x, y), 1.0f + 0x1p-20f);
+    if (!(fabsf(pu) < 0x1p19f)) return false;
+    *t = truncf(pu);
+    return true;
+}
+__device__ __forceinline__ bool trunc_quot_approx(double x, double y, double* t) {
+    const double ay = fabs(y);
+    if (!(ay >= 0x1p-125 && ay <= 0x1p125)) return false;
+    float r0f;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r0f) : "f"(__double2float_rn(y)));
+    const double r0 = (double)r0f;
+    const double r1 = __fma_rn(r0, __fma_rn(-y, r0, 1.0), r0);
+    const double pu = __dmul_rn(__dmul_rn(x, r1), 1.0 + 0x1p-38);
+    if (!(fabs(pu) < 0x1p36)) return false;
+    *t = trunc(pu);
+    return true;
+}
 template <int D> __device__ __forceinline__ typename FOps<D>::T float_floor_divide(typename FOps<D>::T x, typename FOps<D>::T y) {
     typedef FOps<D> O;
     typedef typename O::T T;
     if constexpr (D == DT_F32 || D == DT_F64) {
-        // One division: with x, y finite, y != 0 and t = trunc(fl(x / y))
-        // below 2^20 (2^49), x - t*y is exact in one FMA, one repair step
-        // makes t the exact truncated quotient q and r = fmod(x, y), and
+        // One quotient: with x, y finite, y != 0 and t = trunc(fl(x / y))
+        // (or trunc_quot_approx's t where it applies; either is q or q + 1
+        // in magnitude) below 2^20 (2^49), x - t*y is exact in one FMA, one
+        // repair step makes t the exact truncated quotient q and
+        // r = fmod(x, y), and
         // npy_divmod's (x - r) / y then lies within 1/4 of q, so its
         // floor-and-round gives q (q - 1 after the sign fix) exactly; a
         // zero result takes npy_divmod's copysign(0, x / y), the sign of x
         // XOR y. Everything else takes the full sequence.
         if (O::isfin(x) && O::isfin(y) && !O::iszero(y)) {
-            const T t = trunc(O::div(x, y));
+            T t;
+            if (!trunc_quot_approx(x, y, &t)) t = trunc(O::div(x, y));
             if (fabs(t) < (D == DT_F32 ? (T)0x1p20 : (T)0x1p49)) {
                 T r, q = t;
                 if constexpr (D == DT_F32) r = __fmaf_rn(-t, y, x);
@@ -435,7 +464,12 @@ template <int D> __device__ __forceinline__ typename FOps<D>::T float_floor_divi
                 if (q == (T)0) return (O::neg(x) != O::neg(y)) ? (T)-0.0 : (T)0.0;
                 return q;
             }
+            return floor_divide_full<D>(x, y);  // a quotient of 2^20 (2^49) or more
         }
+        // the special values, inline, with floor_divide_full's results for them
+        if (O::isinf_(x) && O::isfin(y) && !O::iszero(y)) return O::nan();
+        if (O::isinf_(y) && O::isfin(x) && !O::iszero(x) && O::neg(x) != O::neg(y)) return O::negone();
+        return O::floor_(O::div(x, y));
     }
     return floor_divide_full<D>(x, y);
 }

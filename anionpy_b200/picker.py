@@ -291,11 +291,153 @@ def stream_sweep(ncalls=10000, seed=7, steps=4, warmup=2):
     return res
 
 
+# ---------------------------------------------------------------------------
+# the in-stream study: labels from mixed sub-streams instead of lone calls
+# ---------------------------------------------------------------------------
+STREAM_WEIGHTS = os.path.join(HERE, "data", "picker_stream.npz")
+
+
+def class_keys(F: np.ndarray) -> list:
+    """Coarse call classes of a feature matrix: call kind, op class, size
+    (log2 of the element count in steps of 3), output width, stride class,
+    vector path, and for reductions the run length (log2 in steps of 4)."""
+    kind = np.argmax(F[:, 8:11], axis=1)
+    opc = np.argmax(F[:, 0:8], axis=1)
+    size = np.clip((F[:, 20] * 20 / 3).astype(int), 0, 7)
+    wout = np.rint(F[:, 13] * 3).astype(int)
+    scl = np.argmax(F[:, 21:25], axis=1)
+    vec = (F[:, 25] > 0.5).astype(int)
+    run = np.where(kind == 0, 0, np.clip((F[:, 17] * 20 / 4).astype(int), 0, 5))
+    return list(zip(kind.tolist(), opc.tolist(), size.tolist(), wout.tolist(), scl.tolist(), vec.tolist(), run.tolist()))
+
+
+def _stream_timer():
+    L = _lib.lib()
+    e0, e1 = ctypes.c_void_p(), ctypes.c_void_p()
+    _lib.check(L.ionp_event_create(ctypes.byref(e0)))
+    _lib.check(L.ionp_event_create(ctypes.byref(e1)))
+
+    def timed(b: Batch, sched, reps=3, warmup=1) -> float:
+        """Device ms of one graph replay of the whole batch, `sched` a
+        schedule index per call."""
+        b.set_schedules(sched)
+        for _ in range(warmup):
+            b.run(graph=True)
+        _lib.check(L.ionp_device_synchronize())
+        _lib.check(L.ionp_event_record(e0, None))
+        for _ in range(reps):
+            b.run(graph=True)
+        _lib.check(L.ionp_event_record(e1, None))
+        _lib.check(L.ionp_device_synchronize())
+        ms = ctypes.c_float()
+        _lib.check(L.ionp_event_elapsed_ms(e0, e1, ctypes.byref(ms)))
+        return ms.value / reps
+    return timed
+
+
+def stream_collect(ncalls, seed, reps=3, log=None):
+    """(features [n, 32], microseconds per call [n, 48]) from one mixed
+    stream: its calls are grouped by `class_keys`, each class is run as a
+    sub-stream of its own distinct calls (persistent kernel, CUDA graph)
+    under every schedule, and each call is labelled with its class's time per
+    call. A call is thus timed among other calls of its kind -- distinct
+    operands, a shared persistent kernel, the tile mix of a real batch --
+    not as many copies of itself."""
+    import anionpy_b200 as ap
+    from . import workloads
+    calls, _ = workloads.mixed_stream(ncalls=ncalls, seed=seed)
+    pools = workloads.DevicePools(ap, pool_elems=1 << 22, seed=seed + 17)
+    b, _ = workloads.build_batch(ap, calls, pools)
+    F = features(b)
+    del b
+    groups = {}
+    for i, k in enumerate(class_keys(F)):
+        groups.setdefault(k, []).append(i)
+    timed = _stream_timer()
+    X = np.zeros((len(calls), NFEAT), np.float32)
+    Y = np.zeros((len(calls), NUM_SCHEDULES), np.float32)
+    t0 = time.time()
+    row = 0
+    for gi, (k, idx) in enumerate(sorted(groups.items())):
+        bs, _ = workloads.build_batch(ap, [calls[i] for i in idx], pools)
+        n = len(idx)
+        per = np.array([timed(bs, np.full(n, s), reps=reps) for s in range(NUM_SCHEDULES)]) * 1000.0 / n
+        X[row: row + n] = F[idx]
+        Y[row: row + n] = per[None, :]
+        row += n
+        del bs
+        if log and (gi + 1) % 20 == 0:
+            log(f"stream {seed}: {gi + 1}/{len(groups)} classes, {time.time() - t0:.0f} s")
+    return X, Y, len(groups)
+
+
+class StreamPicker(SchedulePicker):
+    """The picker trained on in-stream labels: a call leaves the default
+    schedule only when the network predicts at least `margin` less time for
+    another one."""
+
+    def __init__(self, path=STREAM_WEIGHTS, margin=0.03):
+        super().__init__(path)
+        self.margin = margin
+
+    def pick(self, batch: Batch, fallback=False, reps=3, allowed=None) -> np.ndarray:
+        pred = self.predict(features(batch))
+        best = np.argmin(pred, axis=1)
+        gain = pred[np.arange(len(pred)), best] < pred[:, DEFAULT_INDEX] + np.log(1.0 - self.margin)
+        self.fallbacks = 0
+        return np.where(gain, best, DEFAULT_INDEX)
+
+
+def stream_evaluate(picker_: StreamPicker, ncalls, seed, reps=4):
+    """Device ms of a fresh mixed stream under the default schedule, under
+    each uniform schedule's best, and under the picker's per-call picks."""
+    import anionpy_b200 as ap
+    from . import workloads
+    calls, _ = workloads.mixed_stream(ncalls=ncalls, seed=seed)
+    pools = workloads.DevicePools(ap, pool_elems=1 << 22, seed=seed + 17)
+    b, _ = workloads.build_batch(ap, calls, pools)
+    timed = _stream_timer()
+    n = len(b)
+    uniform = {s: timed(b, np.full(n, s), reps=reps) for s in range(NUM_SCHEDULES)}
+    picks = picker_.pick(b)
+    learned = timed(b, picks, reps=reps)
+    default = timed(b, np.full(n, DEFAULT_INDEX), reps=reps)
+    best_s = min(uniform, key=uniform.get)
+    return {"calls": n, "seed": seed, "default_ms": round(default, 3), "learned_ms": round(learned, 3),
+            "best_uniform_schedule": int(best_s), "best_uniform_ms": round(uniform[best_s], 3),
+            "calls_off_default": int(np.sum(picks != DEFAULT_INDEX)),
+            "distinct_schedules": int(len(set(picks.tolist())))}
+
+
+def stream_study(ncalls=10000, train_seeds=(101, 102), eval_seeds=(7, 9), reps=3, epochs=60,
+                 out=STREAM_WEIGHTS, margin=0.03, log=print):
+    Xs, Ys, ncls = [], [], []
+    for sd in train_seeds:
+        X, Y, k = stream_collect(ncalls, sd, reps=reps, log=log)
+        Xs.append(X); Ys.append(Y); ncls.append(k)
+    X, Y = np.concatenate(Xs), np.concatenate(Ys)
+    mlp = Mlp(seed=3)
+    losses = mlp.fit(X, np.log(np.maximum(Y, 1e-3)), epochs=epochs, log=log)
+    lo, hi = X.min(axis=0), X.max(axis=0)
+    os.makedirs(os.path.dirname(out), exist_ok=True)
+    np.savez_compressed(out, params=mlp.params(), nin=NFEAT, hidden=HIDDEN, nout=NUM_SCHEDULES, feat_lo=lo, feat_hi=hi)
+    sp = StreamPicker(out, margin=margin)
+    res = {"train_streams": list(train_seeds), "calls_per_stream": ncalls, "classes": ncls,
+           "final_train_loss": losses[-1], "margin": margin,
+           "eval": [stream_evaluate(sp, ncalls, sd) for sd in eval_seeds]}
+    return res
+
+
 def main():
     ap_ = argparse.ArgumentParser()
     sub = ap_.add_subparsers(dest="cmd", required=True)
     t = sub.add_parser("stream", help="time the mixed stream under every schedule")
     t.add_argument("--calls", type=int, default=10000)
+    ss = sub.add_parser("stream-study", help="train the picker on in-stream labels")
+    ss.add_argument("--calls", type=int, default=10000)
+    ss.add_argument("--epochs", type=int, default=60)
+    ss.add_argument("--out", default=STREAM_WEIGHTS)
+    ss.add_argument("--report", default=None)
     s = sub.add_parser("study")
     s.add_argument("--train", type=int, default=50000)
     s.add_argument("--test", type=int, default=5000)
@@ -307,6 +449,13 @@ def main():
     args = ap_.parse_args()
     if args.cmd == "stream":
         print(json.dumps(stream_sweep(args.calls), indent=1))
+        return
+    if args.cmd == "stream-study":
+        res = stream_study(args.calls, epochs=args.epochs, out=args.out)
+        print(json.dumps(res, indent=1))
+        if args.report:
+            with open(args.report, "w") as f:
+                json.dump(res, f, indent=1)
         return
     res, data = study(args.train, args.test, reps=args.reps, epochs=args.epochs, out=args.out)
     print(json.dumps(res, indent=1))

@@ -326,14 +326,14 @@ def mixed_stream_bench(ap, L, steps, warmup, ncalls=10000, check_every=10, sched
     if schedules == "learned":
         from anionpy_b200 import picker
         import time as _time
-        if os.path.exists(picker.DEFAULT_WEIGHTS):
+        if os.path.exists(picker.STREAM_WEIGHTS):
+            # the picker trained on in-stream labels, over all 48 schedules
             t0 = _time.perf_counter()
-            sp = picker.SchedulePicker()
-            allowed = picker.stream_schedules()
-            schedules = sp.pick(b, allowed=allowed)
-            res["picker"] = {"pick_s": round(_time.perf_counter() - t0, 3), "fallback_calls": sp.fallbacks,
-                             "distinct_schedules": int(len(set(schedules.tolist()))),
-                             "stream_schedule_set": [int(k) for k in allowed]}
+            sp = picker.StreamPicker()
+            schedules = sp.pick(b)
+            res["picker"] = {"pick_s": round(_time.perf_counter() - t0, 3), "trained_on": "in-stream labels",
+                             "calls_off_default": int(np.sum(schedules != picker.DEFAULT_INDEX)),
+                             "distinct_schedules": int(len(set(schedules.tolist())))}
         else:
             schedules = None
     if schedules is not None:
@@ -623,7 +623,7 @@ def main():
     ap_.add_argument("--elements", type=int, default=N_ELEM, help="elements per operand (default 2^28)")
     ap_.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline leg")
     ap_.add_argument("--no-e2e", action="store_true")
-    ap_.add_argument("--only", default=None, help="run only the cases whose name contains this")
+    ap_.add_argument("--only", default=None, help="run only the cases whose name contains one of these (comma-separated)")
     ap_.add_argument("--no-reduce", action="store_true", help="skip the reduction cases")
     ap_.add_argument("--no-sweep", action="store_true", help="skip the element-wise cases")
     ap_.add_argument("--reduce-scale", type=int, default=1, help="divide the reductions' leading extent (small runs)")
@@ -655,15 +655,16 @@ def main():
     hbm_peak, peak_kind = peaks()
 
     cases, bufs = ([], {}) if args.no_sweep else build_cases(ap, L, n)
-    if args.only:
-        cases = [c for c in cases if args.only in c[0]]
+    only = args.only.split(",") if args.only else None
+    if only:
+        cases = [c for c in cases if any(o in c[0] for o in only)]
     outs = {}
     items = [SweepItem(ap, c, outs) for c in cases]
     red_keep = None
     if not args.no_reduce:
         rcases, red_keep = build_reduce_cases(ap, L, args.reduce_scale)
-        if args.only:
-            rcases = [c for c in rcases if args.only in c.name]
+        if only:
+            rcases = [c for c in rcases if any(o in c.name for o in only)]
         items += rcases
     ev = [ctypes.c_void_p() for _ in range(len(items) + 1)]
     for e in ev:
