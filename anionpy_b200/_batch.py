@@ -64,6 +64,8 @@ class Batch:
         self._keep = []       # operands and outputs stay alive with the batch
         self.outputs = []
         self.kinds = []
+        self._explicit = set()  # calls queued or set with a schedule of their own
+        self._knobs_done = False
 
     def __del__(self):
         try:
@@ -91,6 +93,8 @@ class Batch:
         da, db, do = a._desc(), b._desc(), out._desc()
         check(L.ionp_batch_add_binary(self._h, BINARY_OPS[name], ctypes.byref(da), ctypes.byref(db),
                                       ctypes.byref(do), _sched(sched), ctypes.byref(cid)))
+        if sched is not None:
+            self._explicit.add(cid.value)
         self._keep += [a, b]
         self.outputs.append(out)
         self.kinds.append(("binary", name))
@@ -112,6 +116,8 @@ class Batch:
         da, do = a._desc(), out._desc()
         check(L.ionp_batch_add_reduce(self._h, BINARY_OPS[name], ctypes.byref(da), int(axis), int(bool(keepdims)),
                                       ctypes.byref(do), _sched(sched), ctypes.byref(cid)))
+        if sched is not None:
+            self._explicit.add(cid.value)
         self._keep.append(a)
         self.outputs.append(out)
         self.kinds.append(("reduce", name))
@@ -120,6 +126,33 @@ class Batch:
     def set_schedule(self, call: int, sched) -> None:
         s = sched if isinstance(sched, IonpSchedule) else schedule(int(sched))
         check(lib().ionp_batch_set_schedule(self._h, int(call), ctypes.byref(s)))
+        self._explicit.add(int(call))
+
+    def apply_knobs(self) -> dict:
+        """Apply the run-time knobs (``_config.settings``) to the calls queued
+        without a schedule of their own; done once, before the first run.
+        Returns the settings used."""
+        from ._config import settings
+        cfg = settings()
+        self._knobs_done = True
+        free = [i for i in range(len(self)) if i not in self._explicit]
+        if not free:
+            return cfg
+        L = lib()
+        if cfg["batch_schedule"] is not None:
+            picks = {i: cfg["batch_schedule"] for i in free}
+        elif cfg["batch_picker"] == "stream":
+            from .picker import StreamPicker
+            all_picks = StreamPicker().pick(self)
+            picks = {i: int(all_picks[i]) for i in free}
+        elif cfg["batch_picker"] == "autotune":
+            picks = {i: int(np.argmin(self.time_call(i, reps=3))) for i in free}
+        else:
+            return cfg
+        for i, k in picks.items():
+            s = schedule(k)
+            check(L.ionp_batch_set_schedule(self._h, int(i), ctypes.byref(s)))
+        return cfg
 
     def set_schedules(self, idxs) -> None:
         for i, k in enumerate(idxs):
@@ -127,11 +160,16 @@ class Batch:
 
     # ---- running ----------------------------------------------------------
     def finalize(self, stream=None) -> None:
+        if not self._knobs_done:
+            self.apply_knobs()
         check(lib().ionp_batch_finalize(self._h, stream))
 
     def run(self, graph: bool = True, stream=None) -> None:
         """All calls as one persistent kernel; graph=True replays a captured
-        CUDA graph after the first run."""
+        CUDA graph after the first run. The run-time knobs apply before the
+        first run."""
+        if not self._knobs_done:
+            self.apply_knobs()
         check(lib().ionp_batch_run(self._h, int(bool(graph)), stream))
 
     def run_per_call(self, stream=None) -> None:

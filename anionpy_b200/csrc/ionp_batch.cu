@@ -879,6 +879,7 @@ int32_t ionp_batch_finalize(IonpBatch* b, IonpStream stream) {
 }
 
 int32_t ionp_batch_run(IonpBatch* b, int32_t use_graph, IonpStream stream) {
+    NvtxRange nvtx_("ionp_batch_run");
     int32_t st;
     if (!b) return set_err(IONP_ERR_INVALID, "NULL batch");
     cudaStream_t s = (cudaStream_t)stream;
@@ -902,6 +903,7 @@ int32_t ionp_batch_run(IonpBatch* b, int32_t use_graph, IonpStream stream) {
 }
 
 int32_t ionp_batch_run_per_call(IonpBatch* b, IonpStream stream) {
+    NvtxRange nvtx_("ionp_batch_run_per_call");
     if (!b) return set_err(IONP_ERR_INVALID, "NULL batch");
     for (size_t i = 0; i < b->orig.size(); ++i) {
         IonpBatch::Orig& o = b->orig[i];

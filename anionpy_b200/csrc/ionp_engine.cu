@@ -9,6 +9,7 @@
 #include <mutex>
 #include <sstream>
 #include "ionp_internal.h"
+#include <nvtx3/nvToolsExt.h>
 #include "ionp_host.h"
 #include "ionp_scalar.cuh"
 
@@ -496,6 +497,20 @@ std::atomic<uint64_t> g_launches{0};
 
 void count_launch(int k) { g_launches.fetch_add((uint64_t)k, std::memory_order_relaxed); }
 
+static bool nvtx_enabled() {
+    static const bool on = [] {
+        const char* e = getenv("IONP_NVTX");
+        return e && e[0] == '1';
+    }();
+    return on;
+}
+NvtxRange::NvtxRange(const char* name) : on(nvtx_enabled()) {
+    if (on) nvtxRangePushA(name);
+}
+NvtxRange::~NvtxRange() {
+    if (on) nvtxRangePop();
+}
+
 int sm_count() {
     static std::atomic<int> cache[64];
     int dev = 0;
@@ -915,10 +930,12 @@ static int32_t binary_call(int32_t op, const IonpArr* a, const IonpArr* b, IonpA
 
 int32_t ionp_binary(int32_t op, const IonpArr* a, const IonpArr* b, IonpArr* out, const IonpArr* where, uint32_t* fpe,
                     IonpStream stream) {
+    NvtxRange nvtx_("ionp_binary");
     return binary_call(op, a, b, out, where, fpe, false, stream);
 }
 int32_t ionp_binary_nowait(int32_t op, const IonpArr* a, const IonpArr* b, IonpArr* out, const IonpArr* where,
                            uint32_t* fpe, IonpStream stream) {
+    NvtxRange nvtx_("ionp_binary_nowait");
     return binary_call(op, a, b, out, where, fpe, true, stream);
 }
 
@@ -946,14 +963,17 @@ static int32_t unary_call(int32_t op, const IonpArr* a, IonpArr* out, const Ionp
 }
 
 int32_t ionp_unary(int32_t op, const IonpArr* a, IonpArr* out, const IonpArr* where, uint32_t* fpe, IonpStream stream) {
+    NvtxRange nvtx_("ionp_unary");
     return unary_call(op, a, out, where, fpe, false, stream);
 }
 int32_t ionp_unary_nowait(int32_t op, const IonpArr* a, IonpArr* out, const IonpArr* where, uint32_t* fpe,
                           IonpStream stream) {
+    NvtxRange nvtx_("ionp_unary_nowait");
     return unary_call(op, a, out, where, fpe, true, stream);
 }
 
 int32_t ionp_cast(const IonpArr* a, IonpArr* out, IonpStream stream) {
+    NvtxRange nvtx_("ionp_cast");
     int32_t st;
     if ((st = check_arr(a, "a")) || (st = check_arr(out, "out"))) return st;
     return cast_impl(a, out, nullptr, (cudaStream_t)stream);
@@ -964,6 +984,7 @@ int32_t ionp_cast(const IonpArr* a, IonpArr* out, IonpStream stream) {
 // integer destination is checked; its bounds are the destination's range as
 // float64 (i64::MAX as f64 is 2^63, so 2^63 itself is not flagged).
 int32_t ionp_astype(const IonpArr* a, IonpArr* out, uint32_t* fpe, IonpStream stream) {
+    NvtxRange nvtx_("ionp_astype");
     int32_t st;
     if ((st = check_arr(a, "a")) || (st = check_arr(out, "out"))) return st;
     cudaStream_t s = (cudaStream_t)stream;

@@ -191,6 +191,7 @@ int32_t ionp_cast_scalar(const void* src, int32_t sd, void* dst, int32_t dd) {
 
 int32_t ionp_reduce(int32_t op, const IonpArr* a_in, const int32_t* axes, int32_t naxes, int32_t keepdims,
                     int32_t compute_dtype, const void* initial, const IonpArr* where, IonpArr* out, IonpStream stream) {
+    NvtxRange nvtx_("ionp_reduce");
     int32_t st;
     if ((st = check_arr(a_in, "a")) || (st = check_arr(out, "out"))) return st;
     if (where && (st = check_arr(where, "where"))) return st;
@@ -441,6 +442,7 @@ int32_t ionp_reduce(int32_t op, const IonpArr* a_in, const int32_t* axes, int32_
 }
 
 int32_t ionp_argext(int32_t is_max, const IonpArr* a, int32_t axis, int32_t keepdims, IonpArr* out, IonpStream stream) {
+    NvtxRange nvtx_("ionp_argext");
     int32_t st;
     if ((st = check_arr(a, "a")) || (st = check_arr(out, "out"))) return st;
     if (out->dtype != DT_I64) return set_err(IONP_ERR_TYPE, "argmin/argmax output must be int64");

@@ -58,6 +58,16 @@ MergeOut merge_dims(const MergeIn& in);
 // element-wise cast/copy of a into out with an optional bool mask
 int32_t cast_impl(const IonpArr* a, IonpArr* out, const IonpArr* where, cudaStream_t s);
 
+// --- tracing ------------------------------------------------------------------
+// An NVTX range over the scope (a C-ABI call, a batch run), named after the
+// entry point; on only when the environment sets IONP_NVTX=1 (read once), so
+// a profiler's timeline can show each call, and nothing is done otherwise.
+struct NvtxRange {
+    bool on;
+    explicit NvtxRange(const char* name);
+    ~NvtxRange();
+};
+
 // --- scratch memory from the caching allocator -------------------------------
 void* scratch_alloc(size_t bytes, cudaStream_t s);
 void scratch_free(void* p, cudaStream_t s);

@@ -340,11 +340,13 @@ int32_t fiber_call(int mode, int32_t op, const IonpArr* a, int32_t axis, const i
 using namespace ionp;
 
 extern "C" int32_t ionp_accumulate(int32_t op, const IonpArr* a, int32_t axis, IonpArr* out, IonpStream stream) {
+    NvtxRange nvtx_("ionp_accumulate");
     return fiber_call(0, op, a, axis, nullptr, 0, out, "accumulate", (cudaStream_t)stream);
 }
 
 extern "C" int32_t ionp_reduceat(int32_t op, const IonpArr* a, int32_t axis, const int64_t* indices, int64_t nindices,
                                  IonpArr* out, IonpStream stream) {
+    NvtxRange nvtx_("ionp_reduceat");
     if (nindices < 0 || (nindices > 0 && !indices)) return set_err(IONP_ERR_INVALID, "bad indices");
     return fiber_call(1, op, a, axis, indices, nindices, out, "reduceat", (cudaStream_t)stream);
 }
@@ -632,6 +634,7 @@ static int32_t at_pass(int32_t op, int cd, bool unary, const IonpArr* t, const I
 
 extern "C" int32_t ionp_at(int32_t op, IonpArr* target, const int64_t* indices, int64_t nindices,
                            const IonpArr* values, IonpStream stream) {
+    NvtxRange nvtx_("ionp_at");
     int32_t st;
     if ((st = check_arr(target, "target"))) return st;
     if (values && (st = check_arr(values, "values"))) return st;

@@ -143,3 +143,22 @@ def test_time_call_reports_every_schedule(pools):
         t = b.time_call(call, reps=2)
         assert t.shape == (NUM_SCHEDULES,) and np.all(t > 0) and np.all(np.isfinite(t))
     assert schedule(47).block_tile == 1024 and schedule(47).red_split == 2
+
+
+def test_schedule_knob_applies_and_keeps_results(pools, stream_calls, monkeypatch):
+    """IONP_BATCH_SCHEDULE puts every call queued without a schedule of its
+    own on that schedule at the first run (the tile count matches a batch set
+    to it explicitly), and the results stay those of the default run."""
+    ref, _ = workloads.build_batch(ap, stream_calls, pools)
+    ref.run(graph=False)
+    want = _gets(ref.outputs)
+    explicit, _ = workloads.build_batch(ap, stream_calls, pools)
+    explicit.set_schedules(np.full(len(explicit), 24))
+    explicit.run(graph=False)
+    monkeypatch.setenv("IONP_BATCH_SCHEDULE", "24")
+    b, _ = workloads.build_batch(ap, stream_calls, pools)
+    b.run(graph=True)
+    assert b.info()["tiles"] == explicit.info()["tiles"] != ref.info()["tiles"]
+    got = _gets(b.outputs)
+    for i, c in enumerate(stream_calls):
+        assert_bits_equal(got[i], want[i], f"knob schedule call {i} {c}")
