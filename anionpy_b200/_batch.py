@@ -29,7 +29,7 @@ BLOCK_TILES = (128, 256, 512, 1024)
 VEC_WIDTHS = (1, 2, 4)
 ELEMS_PER_THREAD = (1, 4)
 RED_SPLITS = (1, 2)
-DEFAULT_SCHEDULE = (256, 1, 4, 1)
+DEFAULT_SCHEDULE = (512, 1, 1, 1)  # the C library's default (ionp_batch.cu)
 
 
 def schedule(idx: int) -> IonpSchedule:
@@ -155,8 +155,12 @@ class Batch:
         return cfg
 
     def set_schedules(self, idxs) -> None:
+        """Schedule idxs[i] for call i."""
+        table = [schedule(k) for k in range(NUM_SCHEDULES)]
+        f = lib().ionp_batch_set_schedule
         for i, k in enumerate(idxs):
-            self.set_schedule(i, int(k))
+            check(f(self._h, i, ctypes.byref(table[int(k)])))
+            self._explicit.add(i)
 
     # ---- running ----------------------------------------------------------
     def finalize(self, stream=None) -> None:

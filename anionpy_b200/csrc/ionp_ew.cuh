@@ -46,6 +46,11 @@ template <class R, int N> __device__ __forceinline__ void stv(R* p, int64_t i, c
 // ---------------------------------------------------------------------------
 // binary
 // ---------------------------------------------------------------------------
+// ops whose arithmetic costs more than their memory traffic on this part
+__host__ __device__ constexpr bool ew_heavy_op(int op) {
+    return op == OP_FLOOR_DIVIDE || op == OP_REMAINDER || op == OP_FMOD || op == OP_DIVIDE;
+}
+
 template <int OP, int CD, bool FPE>
 __global__ void __launch_bounds__(EW_THREADS)
 k_bin_contig(const typename DT<CD>::T* __restrict__ a, const typename DT<CD>::T* __restrict__ b,
@@ -59,13 +64,14 @@ k_bin_contig(const typename DT<CD>::T* __restrict__ a, const typename DT<CD>::T*
     const int64_t nvec = n / N;
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    for (; v + (U - 1) * stride < nvec; v += U * stride) {
-        Vec16<T> xa[U], xb[U];
+    auto load = [&](Vec16<T> (&xa)[U], Vec16<T> (&xb)[U], int64_t w) {
 #pragma unroll
         for (int u = 0; u < U; ++u) {
-            if (!a_sc) xa[u] = ldv(a, v + u * stride); else for (int k = 0; k < N; ++k) xa[u].v[k] = a0;
-            if (!b_sc) xb[u] = ldv(b, v + u * stride); else for (int k = 0; k < N; ++k) xb[u].v[k] = b0;
+            if (!a_sc) xa[u] = ldv(a, w + u * stride); else for (int k = 0; k < N; ++k) xa[u].v[k] = a0;
+            if (!b_sc) xb[u] = ldv(b, w + u * stride); else for (int k = 0; k < N; ++k) xb[u].v[k] = b0;
         }
+    };
+    auto compute = [&](const Vec16<T> (&xa)[U], const Vec16<T> (&xb)[U], int64_t w) {
 #pragma unroll
         for (int u = 0; u < U; ++u) {
             R r[N];
@@ -74,7 +80,31 @@ k_bin_contig(const typename DT<CD>::T* __restrict__ a, const typename DT<CD>::T*
                 r[k] = BinOp<OP, CD>::apply(xa[u].v[k], xb[u].v[k]);
                 if constexpr (FPE) bits |= fpe_bits<OP, CD>(xa[u].v[k], xb[u].v[k], r[k]);
             }
-            stv<R, N>(o, v + u * stride, r);
+            stv<R, N>(o, w + u * stride, r);
+        }
+    };
+    if constexpr (ew_heavy_op(OP)) {
+        // arithmetic-heavy ops: the next group's vectors are loaded before
+        // this group is computed, so loads stay in flight through the math
+        Vec16<T> xa[U], xb[U], na[U], nb[U];
+        if (v + (U - 1) * stride < nvec) {
+            load(xa, xb, v);
+            for (;;) {
+                const int64_t vn = v + U * stride;
+                const bool more = vn + (U - 1) * stride < nvec;
+                if (more) load(na, nb, vn);
+                compute(xa, xb, v);
+                v = vn;
+                if (!more) break;
+#pragma unroll
+                for (int u = 0; u < U; ++u) { xa[u] = na[u]; xb[u] = nb[u]; }
+            }
+        }
+    } else {
+        for (; v + (U - 1) * stride < nvec; v += U * stride) {
+            Vec16<T> xa[U], xb[U];
+            load(xa, xb, v);
+            compute(xa, xb, v);
         }
     }
     for (; v < nvec; v += stride) {

@@ -148,17 +148,19 @@ def test_time_call_reports_every_schedule(pools):
 def test_schedule_knob_applies_and_keeps_results(pools, stream_calls, monkeypatch):
     """IONP_BATCH_SCHEDULE puts every call queued without a schedule of its
     own on that schedule at the first run (the tile count matches a batch set
-    to it explicitly), and the results stay those of the default run."""
+    to it explicitly), and each result stays that of the same call launched
+    on its own."""
     ref, _ = workloads.build_batch(ap, stream_calls, pools)
     ref.run(graph=False)
-    want = _gets(ref.outputs)
     explicit, _ = workloads.build_batch(ap, stream_calls, pools)
-    explicit.set_schedules(np.full(len(explicit), 24))
+    explicit.set_schedules(np.full(len(explicit), 16))
     explicit.run(graph=False)
-    monkeypatch.setenv("IONP_BATCH_SCHEDULE", "24")
+    monkeypatch.setenv("IONP_BATCH_SCHEDULE", "16")
     b, _ = workloads.build_batch(ap, stream_calls, pools)
     b.run(graph=True)
     assert b.info()["tiles"] == explicit.info()["tiles"] != ref.info()["tiles"]
     got = _gets(b.outputs)
+    b.run_per_call()
+    want = _gets(b.outputs)
     for i, c in enumerate(stream_calls):
         assert_bits_equal(got[i], want[i], f"knob schedule call {i} {c}")
