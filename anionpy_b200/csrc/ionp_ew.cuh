@@ -46,9 +46,11 @@ template <class R, int N> __device__ __forceinline__ void stv(R* p, int64_t i, c
 // ---------------------------------------------------------------------------
 // binary
 // ---------------------------------------------------------------------------
-// ops whose arithmetic costs more than their memory traffic on this part
-__host__ __device__ constexpr bool ew_heavy_op(int op) {
-    return op == OP_FLOOR_DIVIDE || op == OP_REMAINDER || op == OP_FMOD || op == OP_DIVIDE;
+// 32-bit integer division ops: their loads are issued a group ahead (measured
+// 10 % faster for int32 floor_divide; the same prefetch made the float and
+// 64-bit division family 7-50 % slower, so they keep the plain loop)
+__host__ __device__ constexpr bool ew_prefetch_op(int op, int cd) {
+    return (op == OP_FLOOR_DIVIDE || op == OP_REMAINDER || op == OP_FMOD) && (cd == DT_I32 || cd == DT_U32);
 }
 
 template <int OP, int CD, bool FPE>
@@ -83,9 +85,9 @@ k_bin_contig(const typename DT<CD>::T* __restrict__ a, const typename DT<CD>::T*
             stv<R, N>(o, w + u * stride, r);
         }
     };
-    if constexpr (ew_heavy_op(OP)) {
-        // arithmetic-heavy ops: the next group's vectors are loaded before
-        // this group is computed, so loads stay in flight through the math
+    if constexpr (ew_prefetch_op(OP, CD)) {
+        // the next group's vectors are loaded before this group is
+        // computed, so loads stay in flight through the math
         Vec16<T> xa[U], xb[U], na[U], nb[U];
         if (v + (U - 1) * stride < nvec) {
             load(xa, xb, v);

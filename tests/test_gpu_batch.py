@@ -153,9 +153,9 @@ def test_schedule_knob_applies_and_keeps_results(pools, stream_calls, monkeypatc
     ref, _ = workloads.build_batch(ap, stream_calls, pools)
     ref.run(graph=False)
     explicit, _ = workloads.build_batch(ap, stream_calls, pools)
-    explicit.set_schedules(np.full(len(explicit), 16))
+    explicit.set_schedules(np.full(len(explicit), 0))
     explicit.run(graph=False)
-    monkeypatch.setenv("IONP_BATCH_SCHEDULE", "16")
+    monkeypatch.setenv("IONP_BATCH_SCHEDULE", "0")
     b, _ = workloads.build_batch(ap, stream_calls, pools)
     b.run(graph=True)
     assert b.info()["tiles"] == explicit.info()["tiles"] != ref.info()["tiles"]
