@@ -792,15 +792,17 @@ def main():
 
 
 # DRAM bytes moved per algorithmic byte, from ncu captures of the same
-# kernels on 2^24-element cases (dram__bytes_read.sum + dram__bytes_write.sum
-# of one launch over its algorithmic bytes); the traffic of a full-size
-# launch scales with its elements. sin/float64/step2: 268.5 MB read (every
-# other 8-byte element of each sector is skipped, so reads are twice the
-# logical bytes) + 78.1 MB written of 268.4 MB algorithmic; writes still
-# held in the 126 MB L2 when the 2^24-element launch ends are not counted,
-# so at full size the ratio approaches 1.5. add/float32/contig: 134.2 MB
-# read + 29.2 MB written of 201.3 MB (the same L2 effect on writes).
-NCU_TRAFFIC_PER_BYTE = {"sin/float64/step2": 1.2913, "add/float32/contig": 0.8117}
+# kernels (dram__bytes_read.sum + dram__bytes_write.sum of one launch over its
+# algorithmic bytes); the traffic of a full-size launch scales with its
+# elements. At 2^26 elements (inputs above the 126 MB L2):
+# floor_divide/float64/transposed 1074.3 MB read + 504.0 MB written of
+# 1610.6 MB, add/float32/contig 536.9 MB + 231.0 MB of 805.3 MB (the writes
+# still held in L2 when a launch ends are not counted, so the full-size
+# ratio approaches 1.0). sin/float64/step2 at 2^24 elements: 268.5 MB read
+# (a step-2 slice reads every other 8-byte element, so whole sectors are
+# twice the logical bytes) + 78.1 MB written of 268.4 MB.
+NCU_TRAFFIC_PER_BYTE = {"floor_divide/float64/transposed": 0.9800, "add/float32/contig": 0.9536,
+                        "sin/float64/step2": 1.2913}
 
 
 def traffic_of(case, alg_bytes):
