@@ -1298,8 +1298,9 @@ __device__ __forceinline__ void argext_batch(typename DT<CD>::T& best, int64_t& 
 }
 
 // Column scan: task t = (part, output) scans rows [r0, r1) of its output's
-// column in order, loads in batches of 16 held in two register buffers (the
-// next batch issued before the current one is scanned).
+// column in order, loads in batches of 16; for 4-byte and narrower values
+// two register buffers, the next batch issued before the current one is
+// scanned.
 template <int CD, bool MAX>
 __global__ void __launch_bounds__(RED_THREADS) k_argext_col(RedDesc d) {
     typedef ArgPol<CD, MAX> P;
@@ -1319,7 +1320,15 @@ __global__ void __launch_bounds__(RED_THREADS) k_argext_col(RedDesc d) {
         const int64_t i = r0 + 1;
         const int64_t nb = (r1 - i) / U;
         T xa[U], xb[U];
-        if (nb > 0) {
+        if constexpr (sizeof(T) > 4) {
+            // 8-byte values: one batch at a time (a second buffer cost more
+            // in occupancy than it gained in loads in flight)
+            for (int64_t b = 0; b < nb; ++b) {
+#pragma unroll
+                for (int u = 0; u < U; ++u) xa[u] = p[(i + b * U + u) * d.ws];
+                argext_batch<CD, MAX, U>(best, bi, xa, i + b * U);
+            }
+        } else if (nb > 0) {
 #pragma unroll
             for (int u = 0; u < U; ++u) xa[u] = p[(i + u) * d.ws];
             int64_t b = 0;

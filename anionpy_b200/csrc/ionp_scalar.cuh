@@ -520,13 +520,18 @@ template <class I> __device__ __forceinline__ I w_mul(I x, I y) {
 }
 // Truncated quotient of 64-bit magnitudes (uy != 0). A 64-bit division is a
 // long emulated sequence on the GPU; this one needs it only for quotients of
-// 2^20 or more. Below that, fq = rz(rz(ux) * rcp_rz(ru(uy))) never exceeds
-// ux / uy (every rounding is toward it) and is within a relative 2^-21 of
-// it, so trunc(fq) is the exact quotient or at most one or two below; the
-// remainder ux - q uy (no underflow: q uy <= ux) then repairs q exactly.
+// 2^20 or more. Below that, fq = rn(rn(rz(ux) * rcp~(ru(uy))) * (1 - 2^-20)),
+// rcp~ the hardware reciprocal approximation (within 2^-22 relative): rz(ux)
+// <= ux and ru(uy) >= uy, so fq stays below ux / uy -- the scale by
+// (1 - 2^-20) outweighs the approximation and the two roundings -- and
+// within a relative 1.5 x 2^-20 of it, so trunc(fq) is the exact quotient or
+// at most one or two below; the remainder ux - q uy (no underflow: q uy <=
+// ux) then repairs q exactly.
 __device__ __forceinline__ uint64_t udiv64_trunc(uint64_t ux, uint64_t uy) {
     if (ux < uy) return 0;
-    const float fq = __fmul_rz(__ull2float_rz(ux), __frcp_rz(__ull2float_ru(uy)));
+    float rc;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(rc) : "f"(__ull2float_ru(uy)));
+    const float fq = __fmul_rn(__fmul_rn(__ull2float_rz(ux), rc), 1.0f - 0x1p-20f);
     if (fq < 0x1p20f) {
         uint64_t q = (uint64_t)fq;
         uint64_t r = ux - q * uy;

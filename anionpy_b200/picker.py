@@ -390,9 +390,9 @@ class StreamPicker(SchedulePicker):
         return np.argmin(self.predict(features(batch)), axis=1)
 
 
-def stream_evaluate(picker_: StreamPicker, ncalls, seed, reps=4):
+def stream_evaluate(picker_, ncalls, seed, reps=4):
     """Device ms of a fresh mixed stream under the default schedule, under
-    each uniform schedule's best, and under the picker's per-call picks."""
+    the best single schedule, and (picker_ given) under its per-call picks."""
     import anionpy_b200 as ap
     from . import workloads
     calls, _ = workloads.mixed_stream(ncalls=ncalls, seed=seed)
@@ -401,14 +401,16 @@ def stream_evaluate(picker_: StreamPicker, ncalls, seed, reps=4):
     timed = _stream_timer()
     n = len(b)
     uniform = {s: timed(b, np.full(n, s), reps=reps) for s in range(NUM_SCHEDULES)}
-    picks = picker_.pick(b)
-    learned = timed(b, picks, reps=reps)
     default = timed(b, np.full(n, DEFAULT_INDEX), reps=reps)
     best_s = min(uniform, key=uniform.get)
-    return {"calls": n, "seed": seed, "default_ms": round(default, 3), "learned_ms": round(learned, 3),
-            "best_uniform_schedule": int(best_s), "best_uniform_ms": round(uniform[best_s], 3),
-            "calls_off_default": int(np.sum(picks != DEFAULT_INDEX)),
-            "distinct_schedules": int(len(set(picks.tolist())))}
+    res = {"calls": n, "seed": seed, "default_ms": round(default, 3),
+           "best_uniform_schedule": int(best_s), "best_uniform_ms": round(uniform[best_s], 3)}
+    if picker_ is not None:
+        picks = picker_.pick(b)
+        res.update({"learned_ms": round(timed(b, picks, reps=reps), 3),
+                    "calls_off_default": int(np.sum(picks != DEFAULT_INDEX)),
+                    "distinct_schedules": int(len(set(picks.tolist())))})
+    return res
 
 
 def stream_study(ncalls=10000, train_seeds=(101, 102), eval_seeds=(7, 9, 13), reps=3, epochs=60,
