@@ -387,8 +387,13 @@ k_bin_trv(EwDesc d, uint32_t* flags) {
 // read straight into registers at the output's positions; and both
 // operands of the next tile are loaded while this tile is computed, so each
 // thread keeps one tile of loads in flight through the arithmetic.
+// the 8-byte division family is register-heavy: ask for four resident CTAs
+template <int OP, int CD> constexpr int trv1_min_ctas() {
+    return (sizeof(typename DT<CD>::T) == 8 && (OP == OP_FLOOR_DIVIDE || OP == OP_REMAINDER || OP == OP_FMOD)) ? 4 : 1;
+}
+
 template <int OP, int CD, bool FPE>
-__global__ void __launch_bounds__(EW_THREADS)
+__global__ void __launch_bounds__(EW_THREADS, trv1_min_ctas<OP, CD>())
 k_bin_trv1(EwDesc d, uint32_t* flags) {
     typedef typename DT<CD>::T T;
     typedef BinOp<OP, CD> Op;

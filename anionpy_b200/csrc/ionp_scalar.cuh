@@ -466,10 +466,24 @@ template <int D> __device__ __forceinline__ typename FOps<D>::T float_floor_divi
             }
             return floor_divide_full<D>(x, y);  // a quotient of 2^20 (2^49) or more
         }
-        // the special values, inline, with floor_divide_full's results for them
-        if (O::isinf_(x) && O::isfin(y) && !O::iszero(y)) return O::nan();
-        if (O::isinf_(y) && O::isfin(x) && !O::iszero(x) && O::neg(x) != O::neg(y)) return O::negone();
-        return O::floor_(O::div(x, y));
+        // The special values, inline and without a division: the results
+        // floor_divide_full gives them, case by case (a NaN operand: the
+        // first NaN, quieted; a zero divisor: 0/0 the default NaN, else an
+        // infinity of the quotient's sign; an infinite dividend: NaN, the
+        // default one when the divisor is infinite too; an infinite
+        // divisor: -1 when x is nonzero with the other sign, else a zero of
+        // the quotient's sign).
+        if (O::isnan_(x)) return O::floor_(x);
+        if (O::isnan_(y)) return O::floor_(y);
+        const bool sq = O::neg(x) != O::neg(y);
+        T dn;  // the default NaN of 0/0 and inf/inf
+        if constexpr (D == DT_F32) dn = dnan_f(); else dn = dnan_d();
+        if (O::iszero(y)) return O::iszero(x) ? dn : (sq ? -(T)INFINITY : (T)INFINITY);
+        if (O::isinf_(x)) return O::isinf_(y) ? dn : O::nan();
+        if (!O::iszero(x) && sq) return O::negone();
+        // a zero with the sign of x XOR y, built from the bits
+        if constexpr (D == DT_F32) return bf((fb(x) ^ fb(y)) & 0x80000000u);
+        else return bd((db(x) ^ db(y)) & 0x8000000000000000ull);
     }
     return floor_divide_full<D>(x, y);
 }
