@@ -470,6 +470,28 @@ __global__ void __launch_bounds__(RED_THREADS) k_red_row_top(RedDesc d) {
     }
 }
 
+// Top of a split with at most 32 parts of an order-dependent fold (float
+// add): one thread per output folds its 2^K partials as the perfect tree the
+// K split levels form, left operand first, all loads independent (the tree
+// unrolled at compile time), and applies the seed.
+template <class P, int K> struct TopTree {
+    static __device__ __forceinline__ typename P::A go(const typename P::A* p) {
+        if constexpr (K == 0) return p[0];
+        else return P::fold(TopTree<P, K - 1>::go(p), TopTree<P, K - 1>::go(p + (1 << (K - 1))));
+    }
+};
+template <int OP, int CD, int K>
+__global__ void __launch_bounds__(RED_THREADS) k_red_row_top_tree(RedDesc d) {
+    typedef RPol<OP, CD> P;
+    typedef typename P::A A;
+    for (int64_t o = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; o < d.nout; o += (int64_t)gridDim.x * blockDim.x) {
+        const A v = TopTree<P, K>::go(reinterpret_cast<const A*>(d.scratch) + (o << K));
+        int64_t in_off, out_off;
+        kept_offsets(d, o, &in_off, &out_off);
+        store_cast<CD>(d.o, out_off, d.odt, P::finish(v, d.has_seed, d.seed));
+    }
+}
+
 // Top of a split with few parts of an order-free fold: one thread per
 // output folds its 2^K partials left to right (equal to the tree for these
 // ops) and applies the seed.

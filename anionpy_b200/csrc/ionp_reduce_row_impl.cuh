@@ -42,6 +42,22 @@ static cudaError_t row_top_t(const RedDesc& d, cudaStream_t s) {
             return cudaGetLastError();
         }
     }
+    if constexpr (!red_assoc(OP, CD)) {
+        // many outputs of few parts: one thread per output, the tree unrolled
+        if (d.K >= 1 && d.K <= 5 && d.nout >= sm_count() * 8) {
+            int64_t g = (d.nout + RED_THREADS - 1) / RED_THREADS;
+            if (g > sm_count() * 16) g = sm_count() * 16;
+            switch (d.K) {
+                case 1: k_red_row_top_tree<OP, CD, 1><<<(int)g, RED_THREADS, 0, s>>>(d); break;
+                case 2: k_red_row_top_tree<OP, CD, 2><<<(int)g, RED_THREADS, 0, s>>>(d); break;
+                case 3: k_red_row_top_tree<OP, CD, 3><<<(int)g, RED_THREADS, 0, s>>>(d); break;
+                case 4: k_red_row_top_tree<OP, CD, 4><<<(int)g, RED_THREADS, 0, s>>>(d); break;
+                default: k_red_row_top_tree<OP, CD, 5><<<(int)g, RED_THREADS, 0, s>>>(d); break;
+            }
+            count_launch();
+            return cudaGetLastError();
+        }
+    }
     if (d.K > 2 * TOP_CHUNK_LOG) return cudaErrorInvalidValue;   // planners cap K far below this
     const size_t smem = row_top_smem<A>(d.K);                    // at most 32 KiB
     int grid = (int)(d.nout < sm_count() * 8 ? d.nout : sm_count() * 8);

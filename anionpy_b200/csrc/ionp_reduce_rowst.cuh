@@ -814,6 +814,12 @@ __global__ void __launch_bounds__(32 * PW32_WARPS) k_red_pw32(RedDesc d) {
     };
     for (int s = 0; s < PW32_STAGES - 1; ++s) issue();
     int top = 0;  // stack entries (lane 0)
+    // Once the unit's stack holds a NaN, every window to its right is
+    // irrelevant: all entries left of it are numbers, so each later node
+    // takes the NaN from its left side. The unit's sum is then that NaN, and
+    // its remaining windows are only waited for, not folded.
+    bool unit_nan = false;  // warp-uniform
+    float unit_val = 0.0f;  // lane 0
     int64_t q = 0;
     for (int64_t ui = 0; ui < myunits; ++ui) {
         for (int64_t j = 0; j < wpu; ++j, ++q) {
@@ -825,6 +831,24 @@ __global__ void __launch_bounds__(32 * PW32_WARPS) k_red_pw32(RedDesc d) {
                 for (int64_t q2 = q + 1; q2 < iq; ++q2)
                     if (!mbar_wait_bounded(&bar[q2 % PW32_STAGES], (unsigned)((q2 / PW32_STAGES) & 1))) break;
                 return;
+            }
+            if (unit_nan) {
+                __syncwarp();
+                if (j == wpu - 1) {
+                    if (lane == 0) {
+                        const int64_t u = gw + ui * GW;
+                        top = 0;
+                        if (d.K == 0) {
+                            int64_t in_off, out_off;
+                            kept_offsets(d, u, &in_off, &out_off);
+                            store_cast<CD>(d.o, out_off, d.odt, P::finish(unit_val, d.has_seed, d.seed));
+                        } else {
+                            reinterpret_cast<float*>(d.scratch)[u] = unit_val;
+                        }
+                    }
+                    unit_nan = false;
+                }
+                continue;
             }
             // lane l holds leaf (l % G) * LPG + l / G: the 8 lanes of each
             // 16-byte shared load phase read 8 different groups, whose
@@ -842,19 +866,33 @@ __global__ void __launch_bounds__(32 * PW32_WARPS) k_red_pw32(RedDesc d) {
             float leaf = __fadd_rn(__fadd_rn(__fadd_rn(r[0], r[1]), __fadd_rn(r[2], r[3])),
                                    __fadd_rn(__fadd_rn(r[4], r[5]), __fadd_rn(r[6], r[7])));
             if (leaf != leaf) {
-                // Only the first NaN chain needs the exact replay: in the
+                // Only the first NaN chain needs its exact value: in the
                 // left-first combine tree it is left of every later chain
                 // at their common node, so a later NaN never wins; earlier
                 // chains are NaN-free and exact, and an inf - inf among
-                // them is redone by the exact combine below.
+                // them is redone by the exact combine below. The engine's
+                // sequential add keeps the first NaN it meets, so the chain
+                // is the first NaN element quieted -- or the default NaN
+                // when the plain sum of the elements before it already
+                // turned NaN (inf - inf) -- found without a sequential
+                // replay of the engine's add.
                 int kf = 7;
 #pragma unroll
                 for (int k = 6; k >= 0; --k) kf = (r[k] != r[k]) ? k : kf;
-                float acc = lp[kf];
-#pragma unroll 1
-                for (int i = 1; i < 16; ++i) acc = P::fold(acc, lp[kf + 8 * i]);
+                float xc[16];
 #pragma unroll
-                for (int k = 0; k < 8; ++k) r[k] = (k == kf) ? acc : r[k];
+                for (int i = 0; i < 16; ++i) xc[i] = lp[kf + 8 * i];
+                int i0 = 16;
+#pragma unroll
+                for (int i = 15; i >= 0; --i) i0 = (xc[i] != xc[i]) ? i : i0;
+                float pre = xc[0];
+#pragma unroll
+                for (int i = 1; i < 16; ++i) pre = (i < i0) ? __fadd_rn(pre, xc[i]) : pre;
+                float chain = dnan_f();  // an inf - inf before any NaN element
+#pragma unroll
+                for (int i = 0; i < 16; ++i) chain = (i == i0 && !(i > 0 && pre != pre)) ? quiet_f(xc[i]) : chain;
+#pragma unroll
+                for (int k = 0; k < 8; ++k) r[k] = (k == kf) ? chain : r[k];
                 leaf = P::fold(P::fold(P::fold(r[0], r[1]), P::fold(r[2], r[3])),
                                P::fold(P::fold(r[4], r[5]), P::fold(r[6], r[7])));
             }
@@ -878,6 +916,7 @@ __global__ void __launch_bounds__(32 * PW32_WARPS) k_red_pw32(RedDesc d) {
                     if ((L & (2 * h - 1)) == 0) v = P::fold(v, o);
                 }
             }
+            bool top_nan = false;
             if (lane == 0) {
                 if (wpu == 1) {
                     stk[0] = v;
@@ -890,6 +929,8 @@ __global__ void __launch_bounds__(32 * PW32_WARPS) k_red_pw32(RedDesc d) {
                         stk_h[top - 2] += 1;
                         --top;
                     }
+                    unit_val = stk[top - 1];
+                    top_nan = unit_val != unit_val;
                 }
                 if (j == wpu - 1) {
                     const int64_t u = gw + ui * GW;
@@ -904,6 +945,8 @@ __global__ void __launch_bounds__(32 * PW32_WARPS) k_red_pw32(RedDesc d) {
                     }
                 }
             }
+            // a NaN on the stack settles the rest of the unit
+            unit_nan = __shfl_sync(0xffffffffu, (int)top_nan, 0) != 0 && j != wpu - 1;
         }
     }
 }

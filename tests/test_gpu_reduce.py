@@ -355,3 +355,42 @@ def test_float32_power_of_two_runs(shape, axis):
         want = np.asarray(O.reduce("add", v, axis=1))
         got = ap.add.reduce(ap.from_numpy(c)[:, 1:], axis=1)
         assert_bits_equal(got.get(), want, f"float32 add.reduce misaligned {shape}")
+
+
+def test_float32_window_nan_rules():
+    """Hand-placed NaN patterns for the float32 window kernel's shortcuts: a
+    chain whose inf - inf comes before its first NaN element (default NaN),
+    a NaN in a chain's first element, a NaN after an infinity, a chain with
+    an inf - inf and no NaN element, several NaN payloads in one row (the
+    leftmost must win), and a NaN early in a row followed by other NaNs in
+    later windows (the rest of the unit is skipped)."""
+    f = lambda u: np.array([u], np.uint32).view(np.float32)[0]
+    rows, w = 12, 1 << 15
+    a = np.random.default_rng(5).standard_normal((rows, w), dtype=np.float32)
+    def at(r, leaf, chain, i):            # element i of chain `chain` of leaf `leaf`
+        return r, 128 * leaf + chain + 8 * i
+    # row 0: inf, -inf then a NaN in the same chain -> the default NaN wins
+    a[at(0, 3, 2, 1)] = np.inf; a[at(0, 3, 2, 4)] = -np.inf; a[at(0, 3, 2, 9)] = f(0x7FC0AAAA)
+    # row 1: NaN in element 0 of a chain, another NaN later in it
+    a[at(1, 0, 5, 0)] = f(0x7FC01111); a[at(1, 0, 5, 7)] = f(0xFFC02222)
+    # row 2: infinity then a NaN (no inf - inf): the NaN, quieted
+    a[at(2, 7, 0, 2)] = np.inf; a[at(2, 7, 0, 3)] = f(0x7F800005)
+    # row 3: inf - inf and no NaN element in the chain
+    a[at(3, 31, 7, 14)] = np.inf; a[at(3, 31, 7, 15)] = -np.inf
+    # row 4: NaNs of different payloads in different leaves and windows
+    a[at(4, 40, 1, 3)] = f(0xFFC03333); a[at(4, 2, 6, 12)] = f(0x7FC04444); a[4, 20000] = f(0x7FC05555)
+    # row 5: a NaN in the first window, other NaNs in every later window
+    a[5, 100] = f(0x7FC06666)
+    for k in range(1, 8):
+        a[5, 4096 * k + 7] = f(0xFFC07777 + k)
+    # row 6: +inf in one window, -inf in a later one: default NaN at a node
+    a[6, 10] = np.inf; a[6, 30000] = -np.inf
+    # row 7: several NaN chains in one leaf, the later ones with other payloads
+    a[at(7, 5, 1, 8)] = f(0x7FC08888); a[at(7, 5, 2, 0)] = f(0x7FC09999); a[at(7, 5, 6, 3)] = f(0xFF800123)
+    # row 8: a NaN in the last window only
+    a[8, w - 3] = f(0x7FC0ABCD)
+    for axis in (1, None):
+        want = np.asarray(O.reduce("add", a, axis=axis))
+        got = ap.add.reduce(ap.from_numpy(a), axis=axis)
+        assert_bits_equal(np.asarray(got.get() if isinstance(got, ap.ndarray) else got).reshape(want.shape), want,
+                          f"window NaN rules axis={axis}")
