@@ -1152,9 +1152,9 @@ __global__ void __launch_bounds__(RED_THREADS) k_argext(RedDesc d) {
             auto take = [&](const T (&x)[VE], int64_t e0) {
                 bool nan = false;
                 if constexpr (dt_is_float(CD)) {
+                    if (bi >= 0 && P::is_nan(best)) return;  // nothing beats a NaN that came first
 #pragma unroll
                     for (int k = 0; k < VE; ++k) nan |= P::is_nan(x[k]);
-                    nan |= bi >= 0 && P::is_nan(best);
                 }
                 if (CD != DT_F16 && bi >= 0 && !nan) {
 #pragma unroll
@@ -1305,9 +1305,9 @@ __device__ __forceinline__ void argext_batch(typename DT<CD>::T& best, int64_t& 
     typedef ArgPol<CD, MAX> P;
     bool nan = false;
     if constexpr (dt_is_float(CD)) {
+        if (P::is_nan(best)) return;  // nothing beats a NaN that came first
 #pragma unroll
         for (int u = 0; u < U; ++u) nan |= P::is_nan(x[u]);
-        nan |= P::is_nan(best);
     }
     if (CD != DT_F16 && !nan) {
 #pragma unroll
