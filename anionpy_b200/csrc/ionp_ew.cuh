@@ -387,9 +387,12 @@ k_bin_trv(EwDesc d, uint32_t* flags) {
 // read straight into registers at the output's positions; and both
 // operands of the next tile are loaded while this tile is computed, so each
 // thread keeps one tile of loads in flight through the arithmetic.
-// the 8-byte division family is register-heavy: ask for four resident CTAs
+// the division family is register-heavy (112 registers for 4-byte types
+// unbounded, two resident CTAs): ask for three resident CTAs for 4-byte
+// types and four for 8-byte types
 template <int OP, int CD> constexpr int trv1_min_ctas() {
-    return (sizeof(typename DT<CD>::T) == 8 && (OP == OP_FLOOR_DIVIDE || OP == OP_REMAINDER || OP == OP_FMOD)) ? 4 : 1;
+    return (OP == OP_FLOOR_DIVIDE || OP == OP_REMAINDER || OP == OP_FMOD)
+        ? (sizeof(typename DT<CD>::T) == 8 ? 4 : 3) : 1;
 }
 
 template <int OP, int CD, bool FPE>

@@ -101,47 +101,83 @@ __device__ __forceinline__ double x_floor(double x) { return isnan_d(x) ? quiet_
 __device__ __forceinline__ float x_sqrt(float x) { return isnan_f(x) ? quiet_f(x) : (x < 0.0f ? dnan_f() : __fsqrt_rn(x)); }
 __device__ __forceinline__ double x_sqrt(double x) { return isnan_d(x) ? quiet_d(x) : (x < 0.0 ? dnan_d() : __dsqrt_rn(x)); }
 
+// The common case of fmod, remainder and floor_divide without a branch:
+// x finite, 2^-125 <= |y| <= 2^125 and |x / y| below 2^19 (float32) or 2^36
+// (float64); quot_fast returns false for every other input, whose outputs
+// t and m are then meaningless. p, the quotient from a reciprocal
+// approximation scaled up by 2^-20 (2^-38), is at least |x / y| and less
+// than |x / y| + 1 in magnitude:
+//  float32: rcp.approx is within 1 ulp (2^-23 relative) and the two
+//    products round by 2^-24 each, so the relative error of p is inside
+//    (2^-20 - 2^-22, 2^-20 + 2^-22), below 2^-19 / |x / y|;
+//  float64: the float32 reciprocal of y rounded to float32 is within
+//    2^-22.4, one Newton step r1 = r0 + r0 (1 - y r0) squares that to
+//    below 2^-44, and the two products round by 2^-53 each.
+// So t = trunc(p) is the exact truncated quotient q or q + 1 in magnitude,
+// and m = x - t y is exact in one fused multiply-add: it is the true
+// remainder when t = q, and the true remainder less y (towards zero, with
+// the other sign, never zero) when t is one too large; Sterbenz's lemma
+// covers the |x| < |y| case, and otherwise m is a multiple of y's last
+// place below |y|.
+__device__ __forceinline__ bool quot_fast(float x, float y, float* t, float* m) {
+    const uint32_t ax = fb(x) & 0x7FFFFFFFu, ay = fb(y) & 0x7FFFFFFFu;
+    float rc;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(rc) : "f"(y));
+    const float p = __fmul_rn(__fmul_rn(x, rc), 1.0f + 0x1p-20f);
+    *t = truncf(p);
+    *m = __fmaf_rn(-*t, y, x);
+    // 0x01000000 = 2^-125, 0x7E000000 = 2^125
+    return (ax < 0x7F800000u) & (ay - 0x01000000u <= 0x7D000000u) & (fabsf(p) < 0x1p19f);
+}
+__device__ __forceinline__ bool quot_fast(double x, double y, double* t, double* m) {
+    const uint64_t ax = db(x) & 0x7FFFFFFFFFFFFFFFull, ay = db(y) & 0x7FFFFFFFFFFFFFFFull;
+    float r0f;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r0f) : "f"(__double2float_rn(y)));
+    const double r0 = (double)r0f;
+    const double r1 = __fma_rn(r0, __fma_rn(-y, r0, 1.0), r0);
+    const double p = __dmul_rn(__dmul_rn(x, r1), 1.0 + 0x1p-38);
+    *t = trunc(p);
+    *m = __fma_rn(-*t, y, x);
+    // 0x3820000000000000 = 2^-125, 0x47C0000000000000 = 2^125
+    return (ax < 0x7FF0000000000000ull) & (ay - 0x3820000000000000ull <= 0x0FA0000000000000ull) & (fabs(p) < 0x1p36);
+}
 // glibc fmod semantics (what Rust's float `%` calls): NaN operands propagate,
 // fmod(inf, y) and fmod(x, 0) are the default NaN, fmod(x, inf) = x.
-// Quotients below 2^23 (2^52): q = trunc(fl(x / y)) is the exact truncated
-// quotient or one too large in magnitude (rounding is monotone and every
-// integer below 2^24 is representable), x - q y is exact in one fused
-// multiply-add (the true remainder is representable; the one-too-large case
-// is within a factor two of y, so Sterbenz applies), and adding y back with
-// x's sign repairs the one-too-large case exactly. Larger quotients take the
+// quot_fast's case inline: m, with y added back (x's sign) when t was one
+// too large, which is exact. The rest out of line: for quotients below 2^23
+// (2^52) q = trunc(fl(x / y)) is again the truncated quotient or one too
+// large (rounding is monotone and every integer below 2^24 is
+// representable) and the same repair applies; larger quotients take the
 // library's fmod.
-// the special values and the huge-quotient case, out of line
-// quotients of 2^23 (2^52) and more, out of line
-static __device__ __noinline__ float x_fmod_big(float x, float y) { return fmodf(x, y); }
-static __device__ __noinline__ double x_fmod_big(double x, double y) { return fmod(x, y); }
-__device__ __forceinline__ float x_fmod(float x, float y) {
-    if (isfinite(x) && isfinite(y) && y != 0.0f) {
-        const float q = truncf(__fdiv_rn(x, y));
-        if (fabsf(q) < 0x1p23f) {
-            float r = __fmaf_rn(-q, y, x);
-            if (r != 0.0f && signbit(r) != signbit(x)) r = __fadd_rn(r, copysignf(y, x));
-            return r == 0.0f ? copysignf(0.0f, x) : r;
+template <class F> static __device__ __noinline__ F x_fmod_slow(F x, F y) {
+    if (isfinite(x) && isfinite(y) && y != (F)0) {
+        F q;
+        if constexpr (sizeof(F) == 4) q = truncf(__fdiv_rn(x, y));
+        else q = trunc(__ddiv_rn(x, y));
+        if (fabs(q) < (sizeof(F) == 4 ? (F)0x1p23 : (F)0x1p52)) {
+            F r;
+            if constexpr (sizeof(F) == 4) r = __fmaf_rn(-q, y, x);
+            else r = __fma_rn(-q, y, x);
+            if (r != (F)0 && signbit(r) != signbit(x)) r = r + copysign(y, x);
+            return r == (F)0 ? copysign((F)0, x) : r;
         }
-        return x_fmod_big(x, y);
+        if constexpr (sizeof(F) == 4) return fmodf(x, y);
+        else return fmod(x, y);
     }
-    // the special values, inline (a call here costs every warp that meets one)
-    if (isnan_f(x) || isnan_f(y)) return nan2(x, y);
-    if (isinf(x) || y == 0.0f) return dnan_f();
+    if (x != x || y != y) return nan2(x, y);
+    if (isinf(x) || y == (F)0) {
+        if constexpr (sizeof(F) == 4) return dnan_f();
+        else return dnan_d();
+    }
     return x;  // y infinite, x finite
 }
-__device__ __forceinline__ double x_fmod(double x, double y) {
-    if (isfinite(x) && isfinite(y) && y != 0.0) {
-        const double q = trunc(__ddiv_rn(x, y));
-        if (fabs(q) < 0x1p52) {
-            double r = __fma_rn(-q, y, x);
-            if (r != 0.0 && signbit(r) != signbit(x)) r = __dadd_rn(r, copysign(y, x));
-            return r == 0.0 ? copysign(0.0, x) : r;
-        }
-        return x_fmod_big(x, y);
+template <class F> __device__ __forceinline__ F x_fmod(F x, F y) {
+    F t, m;
+    if (quot_fast(x, y, &t, &m)) {
+        const F r = (m != (F)0 && signbit(m) != signbit(x)) ? m + copysign(y, x) : m;
+        return r == (F)0 ? copysign((F)0, x) : r;
     }
-    if (isnan_d(x) || isnan_d(y)) return nan2(x, y);
-    if (isinf(x) || y == 0.0) return dnan_d();
-    return x;
+    return x_fmod_slow(x, y);
 }
 
 // ---------------------------------------------------------------------------
@@ -408,82 +444,67 @@ template <int D> static __device__ __noinline__ typename FOps<D>::T floor_divide
     }
     return O::floor_(O::div(x, y));
 }
-// trunc(x / y) or one more in magnitude, from an approximate quotient, for
-// x finite and 2^-125 <= |y| <= 2^125; false when |x / y| is too large.
-// float32: __fdividef is within 2 ulps here; scaled up by 2^-20 the quotient
-// is at least |x / y| and, below 2^19, less than q + 2 (q = trunc|x / y|).
-// float64: a float32 reciprocal approximation refined by one Newton step is
-// within a relative 2^-42; scaled up by 2^-38 the same holds below 2^36.
-// Either way t is q or q + 1 in magnitude, which the caller's repair step
-// (exact x - t*y, one correction) turns into q exactly.
-__device__ __forceinline__ bool trunc_quot_approx(float x, float y, float* t) {
-    const float ay = fabsf(y);
-    if (!(ay >= 0x1p-125f && ay <= 0x1p125f)) return false;
-    const float pu = __fmul_rn(__fdividef(x, y), 1.0f + 0x1p-20f);
-    if (!(fabsf(pu) < 0x1p19f)) return false;
-    *t = truncf(pu);
-    return true;
-}
-__device__ __forceinline__ bool trunc_quot_approx(double x, double y, double* t) {
-    const double ay = fabs(y);
-    if (!(ay >= 0x1p-125 && ay <= 0x1p125)) return false;
-    float r0f;
-    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r0f) : "f"(__double2float_rn(y)));
-    const double r0 = (double)r0f;
-    const double r1 = __fma_rn(r0, __fma_rn(-y, r0, 1.0), r0);
-    const double pu = __dmul_rn(__dmul_rn(x, r1), 1.0 + 0x1p-38);
-    if (!(fabs(pu) < 0x1p36)) return false;
-    *t = trunc(pu);
-    return true;
-}
-template <int D> __device__ __forceinline__ typename FOps<D>::T float_floor_divide(typename FOps<D>::T x, typename FOps<D>::T y) {
+// The one-division path and the special values, out of line. With x, y
+// finite, y != 0 and t = trunc(fl(x / y)) (q or q + 1 in magnitude) below
+// 2^20 (2^49), x - t*y is exact in one FMA, one repair step makes t the
+// exact truncated quotient q and r = fmod(x, y), and npy_divmod's
+// (x - r) / y then lies within 1/4 of q, so its floor-and-round gives q
+// (q - 1 after the sign fix) exactly; a zero result takes npy_divmod's
+// copysign(0, x / y), the sign of x XOR y. Larger quotients take the full
+// sequence. The special values take the results floor_divide_full gives
+// them, case by case, without a division (a NaN operand: the first NaN,
+// quieted; a zero divisor: 0/0 the default NaN, else an infinity of the
+// quotient's sign; an infinite dividend: NaN, the default one when the
+// divisor is infinite too; an infinite divisor: -1 when x is nonzero with
+// the other sign, else a zero of the quotient's sign).
+template <int D> static __device__ __noinline__ typename FOps<D>::T floor_divide_slow(typename FOps<D>::T x, typename FOps<D>::T y) {
     typedef FOps<D> O;
     typedef typename O::T T;
-    if constexpr (D == DT_F32 || D == DT_F64) {
-        // One quotient: with x, y finite, y != 0 and t = trunc(fl(x / y))
-        // (or trunc_quot_approx's t where it applies; either is q or q + 1
-        // in magnitude) below 2^20 (2^49), x - t*y is exact in one FMA, one
-        // repair step makes t the exact truncated quotient q and
-        // r = fmod(x, y), and
-        // npy_divmod's (x - r) / y then lies within 1/4 of q, so its
-        // floor-and-round gives q (q - 1 after the sign fix) exactly; a
-        // zero result takes npy_divmod's copysign(0, x / y), the sign of x
-        // XOR y. Everything else takes the full sequence.
-        if (O::isfin(x) && O::isfin(y) && !O::iszero(y)) {
-            T t;
-            if (!trunc_quot_approx(x, y, &t)) t = trunc(O::div(x, y));
-            if (fabs(t) < (D == DT_F32 ? (T)0x1p20 : (T)0x1p49)) {
-                T r, q = t;
-                if constexpr (D == DT_F32) r = __fmaf_rn(-t, y, x);
-                else r = __fma_rn(-t, y, x);
-                if (!O::iszero(r) && O::neg(r) != O::neg(x)) {
-                    r = O::add(r, copysign(y, x));
-                    q = O::sub(q, O::neg(x) == O::neg(y) ? (T)1 : (T)-1);
-                }
-                if (!O::iszero(r) && O::neg(r) != O::neg(y)) q = O::sub(q, (T)1);
-                if (q == (T)0) return (O::neg(x) != O::neg(y)) ? (T)-0.0 : (T)0.0;
-                return q;
+    if (O::isfin(x) && O::isfin(y) && !O::iszero(y)) {
+        const T t = trunc(O::div(x, y));
+        if (fabs(t) < (D == DT_F32 ? (T)0x1p20 : (T)0x1p49)) {
+            T r, q = t;
+            if constexpr (D == DT_F32) r = __fmaf_rn(-t, y, x);
+            else r = __fma_rn(-t, y, x);
+            if (!O::iszero(r) && O::neg(r) != O::neg(x)) {
+                r = O::add(r, copysign(y, x));
+                q = O::sub(q, O::neg(x) == O::neg(y) ? (T)1 : (T)-1);
             }
-            return floor_divide_full<D>(x, y);  // a quotient of 2^20 (2^49) or more
+            if (!O::iszero(r) && O::neg(r) != O::neg(y)) q = O::sub(q, (T)1);
+            if (q == (T)0) return (O::neg(x) != O::neg(y)) ? (T)-0.0 : (T)0.0;
+            return q;
         }
-        // The special values, inline and without a division: the results
-        // floor_divide_full gives them, case by case (a NaN operand: the
-        // first NaN, quieted; a zero divisor: 0/0 the default NaN, else an
-        // infinity of the quotient's sign; an infinite dividend: NaN, the
-        // default one when the divisor is infinite too; an infinite
-        // divisor: -1 when x is nonzero with the other sign, else a zero of
-        // the quotient's sign).
-        if (O::isnan_(x)) return O::floor_(x);
-        if (O::isnan_(y)) return O::floor_(y);
-        const bool sq = O::neg(x) != O::neg(y);
-        T dn;  // the default NaN of 0/0 and inf/inf
-        if constexpr (D == DT_F32) dn = dnan_f(); else dn = dnan_d();
-        if (O::iszero(y)) return O::iszero(x) ? dn : (sq ? -(T)INFINITY : (T)INFINITY);
-        if (O::isinf_(x)) return O::isinf_(y) ? dn : O::nan();
-        if (!O::iszero(x) && sq) return O::negone();
-        // a zero with the sign of x XOR y, built from the bits
-        if constexpr (D == DT_F32) return bf((fb(x) ^ fb(y)) & 0x80000000u);
-        else return bd((db(x) ^ db(y)) & 0x8000000000000000ull);
+        return floor_divide_full<D>(x, y);  // a quotient of 2^20 (2^49) or more
+    }
+    if (O::isnan_(x)) return O::floor_(x);
+    if (O::isnan_(y)) return O::floor_(y);
+    const bool sq = O::neg(x) != O::neg(y);
+    T dn;  // the default NaN of 0/0 and inf/inf
+    if constexpr (D == DT_F32) dn = dnan_f(); else dn = dnan_d();
+    if (O::iszero(y)) return O::iszero(x) ? dn : (sq ? -(T)INFINITY : (T)INFINITY);
+    if (O::isinf_(x)) return O::isinf_(y) ? dn : O::nan();
+    if (!O::iszero(x) && sq) return O::negone();
+    // a zero with the sign of x XOR y, built from the bits
+    if constexpr (D == DT_F32) return bf((fb(x) ^ fb(y)) & 0x80000000u);
+    else return bd((db(x) ^ db(y)) & 0x8000000000000000ull);
+}
+// quot_fast's case inline: npy_divmod's result is then the exact floor of
+// x / y. With m = x - t y, the floor is t - 1 exactly when m is nonzero with
+// the sign opposite to y's: for a positive quotient that is t one too
+// large, and for a negative one a nonzero remainder with t exact; in the
+// other two cases (t exact, or one too large in magnitude below a negative
+// quotient with a nonzero remainder) it is t. A zero result takes the sign
+// of x XOR y. Everything else goes out of line.
+template <int D> __device__ __forceinline__ typename FOps<D>::T float_floor_divide(typename FOps<D>::T x, typename FOps<D>::T y) {
+    typedef typename FOps<D>::T T;
+    if constexpr (D == DT_F32 || D == DT_F64) {
+        T t, m;
+        if (quot_fast(x, y, &t, &m)) {
+            const T f = (m != (T)0 && signbit(m) != signbit(y)) ? t - (T)1 : t;
+            if constexpr (D == DT_F32) return f == 0.0f ? bf((fb(x) ^ fb(y)) & 0x80000000u) : f;
+            else return f == 0.0 ? bd((db(x) ^ db(y)) & 0x8000000000000000ull) : f;
+        }
+        return floor_divide_slow<D>(x, y);
     }
     return floor_divide_full<D>(x, y);
 }

@@ -240,25 +240,38 @@ def test_scalar_operands_and_0d():
     assert isinstance(s, np.float64) and s == 3.5
 
 
+@pytest.mark.parametrize("op", ["floor_divide", "remainder", "fmod"])
 @pytest.mark.parametrize("dt", [np.float32, np.float64], ids=lambda d: np.dtype(d).name)
-def test_float_floor_divide_quotient_edges(dt):
-    """floor_divide at the edges of the one-division path: quotients just
-    below and above 2^20 (float32) / 2^49 (float64), quotients a rounding
-    away from an integer, exact multiples, zeros of both signs and huge
-    quotients, against the oracle's npy_divmod sequence bit for bit."""
+def test_float_division_quotient_edges(op, dt):
+    """floor_divide, remainder and fmod at the edges of their fast paths:
+    quotients just below and above 2^19 / 2^20 / 2^23 (float32) and 2^36 /
+    2^49 / 2^52 (float64), the limits of the approximate quotient and of the
+    one-division paths; quotients a rounding away from an integer, exact
+    multiples, divisors near 2^+-125 (the approximate quotient's range),
+    zeros of both signs and huge quotients, against the oracle bit for
+    bit."""
     rng = np.random.default_rng(77)
-    lim = 2.0 ** 20 if dt == np.float32 else 2.0 ** 49
-    eps = 2.0 ** -23 if dt == np.float32 else 2.0 ** -52
-    n = 40000
+    f32 = dt == np.float32
+    lims = [2.0 ** 19, 2.0 ** 20, 2.0 ** 23] if f32 else [2.0 ** 36, 2.0 ** 49, 2.0 ** 52]
+    eps = 2.0 ** -23 if f32 else 2.0 ** -52
+    n, g = 48000, 6
+    m = n // g
     y = rng.standard_normal(n) * np.exp2(rng.integers(-20, 20, n))
-    q = np.concatenate([rng.integers(1, 64, n // 4), rng.integers(lim // 2, lim * 2, n // 4).astype(np.float64),
-                        rng.integers(1, 1 << 16, n // 4), np.zeros(n - 3 * (n // 4))])
+    q = np.concatenate([rng.integers(1, 64, m).astype(np.float64)]
+                       + [rng.integers(lim // 2, lim * 2, m).astype(np.float64) for lim in lims]
+                       + [rng.integers(1, 1 << 16, n - 4 * m).astype(np.float64)])
+    # divisors at the approximate quotient's range limits, small quotients
+    edge = slice(n - m, n)
+    y[edge] = rng.choice([-1.0, 1.0], m) * rng.uniform(1.0, 2.0, m) * np.exp2(
+        rng.choice([-127, -126, -125, -124, 123, 124, 125], m).astype(np.float64))
+    q[edge] = rng.integers(1, 4, m)
     x = q * y * (1 + rng.choice([-1.0, 0.0, 1.0], n) * eps) * rng.choice([-1.0, 1.0], n)
     x[-100:] = rng.choice([0.0, -0.0], 100)
-    xs, ys = x.astype(dt), y.astype(dt)
-    got = ap.floor_divide(ap.from_numpy(xs), ap.from_numpy(ys)).get()
-    want, _ = O.binary("floor_divide", xs, ys)
-    assert_bits_equal(got, want, f"floor_divide {np.dtype(dt).name} quotient edges")
+    with np.errstate(over="ignore"):
+        xs, ys = x.astype(dt), y.astype(dt)
+    got = getattr(ap, op)(ap.from_numpy(xs), ap.from_numpy(ys)).get()
+    want, _ = O.binary(op, xs, ys)
+    assert_bits_equal(got, want, f"{op} {np.dtype(dt).name} quotient edges")
 
 
 @pytest.mark.parametrize("dt", [np.float32, np.int32, np.uint32, np.float64, np.int64], ids=lambda d: np.dtype(d).name)
