@@ -510,6 +510,60 @@ __global__ void __launch_bounds__(RED_THREADS) k_red_row_top_small(RedDesc d) {
     }
 }
 
+// Signed-integer key of a float's bits, in the order of the values with -0
+// below +0 (NaN excluded), and back.
+__device__ __forceinline__ int32_t fkey(float v) { const int32_t k = (int32_t)fb(v); return k < 0 ? k ^ 0x7FFFFFFF : k; }
+__device__ __forceinline__ int64_t fkey(double v) { const int64_t k = (int64_t)db(v); return k < 0 ? k ^ 0x7FFFFFFFFFFFFFFFll : k; }
+__device__ __forceinline__ float fkey_inv(int32_t k) { return bf((uint32_t)(k < 0 ? k ^ 0x7FFFFFFF : k)); }
+__device__ __forceinline__ double fkey_inv(int64_t k) { return bd((uint64_t)(k < 0 ? k ^ 0x7FFFFFFFFFFFFFFFll : k)); }
+
+// One batch of a column fold in order: float add sums plainly and replays
+// the batch with the engine's NaN rule only when the sum turns NaN (once the
+// accumulator is a quiet NaN no later add changes it); float max/min fold a
+// NaN-free batch as an integer max/min of order keys.
+template <int OP, int CD, int U>
+__device__ __forceinline__ void col_fold_batch(typename DT<CD>::T& acc, const typename DT<CD>::T (&x)[U]) {
+    typedef typename DT<CD>::T T;
+    if constexpr ((OP == OP_MAXIMUM || OP == OP_MINIMUM) && (CD == DT_F32 || CD == DT_F64)) {
+        // Without a NaN, float_max / float_min (ufunc.rs:2402-2436) fold to
+        // the largest / smallest value with -0 below +0 (their tie rule):
+        // an integer max / min of the keys. A batch with a NaN, or a NaN
+        // accumulator, folds element by element with the NaN rules.
+        bool nan = acc != acc;
+#pragma unroll
+        for (int u = 0; u < U; ++u) nan |= x[u] != x[u];
+        if (!nan) {
+            auto k = fkey(acc);
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                const auto ku = fkey(x[u]);
+                k = OP == OP_MAXIMUM ? (ku > k ? ku : k) : (ku < k ? ku : k);
+            }
+            acc = fkey_inv(k);
+        } else {
+#pragma unroll
+            for (int u = 0; u < U; ++u) acc = BinOp<OP, CD>::apply(acc, x[u]);
+        }
+    } else if constexpr (OP == OP_ADD && (CD == DT_F32 || CD == DT_F64)) {
+        if (acc == acc) {
+            T r = acc;
+#pragma unroll
+            for (int u = 0; u < U; ++u) r = plain_sum(r, x[u]);
+            if (r != r) {
+                r = acc;
+#pragma unroll
+                for (int u = 0; u < U; ++u) r = BinOp<OP, CD>::apply(r, x[u]);
+            }
+            acc = r;
+        } else {
+            acc = BinOp<OP, CD>::apply(acc, x[0]);  // quiets a signaling NaN once
+        }
+    } else {
+#pragma unroll
+        for (int u = 0; u < U; ++u) acc = BinOp<OP, CD>::apply(acc, x[u]);
+    }
+}
+
 // COL kernel: sequential fold per output over the narrow dims (fold order),
 // U loads in flight per thread (64 when the outputs are too few for 16 to
 // keep HBM busy).
@@ -517,7 +571,6 @@ template <int OP, int CD, bool CASTLD, int U = 16>
 __global__ void __launch_bounds__(RED_THREADS) k_red_col(RedDesc d) {
     typedef typename DT<CD>::T T;
     typedef RPol<OP, CD, CASTLD> P;
-    constexpr bool FADD = OP == OP_ADD && (CD == DT_F32 || CD == DT_F64);
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     int64_t total = 1;
     for (int k = 0; k < d.nr; ++k) total *= d.rshape[k];
@@ -548,27 +601,10 @@ __global__ void __launch_bounds__(RED_THREADS) k_red_col(RedDesc d) {
                     if constexpr (CASTLD) x[u] = load_int_widen<CD>(d.a, b0 + (j + u) * rs_in, d.adt);
                     else x[u] = ((const T*)d.a)[b0 + (j + u) * rs_in];
                 }
-                if constexpr (FADD) {
-                    // plain adds; a NaN result replays the block with the
-                    // engine's NaN rule; once the sum is a quiet NaN no
-                    // later add changes it
-                    if (acc == acc) {
-                        T r = acc;
-#pragma unroll
-                        for (int u = 0; u < U; ++u) r = plain_sum(r, x[u]);
-                        if (r != r) {
-                            r = acc;
-#pragma unroll
-                            for (int u = 0; u < U; ++u) r = BinOp<OP, CD>::apply(r, x[u]);
-                        }
-                        acc = r;
-                    } else {
-                        acc = BinOp<OP, CD>::apply(acc, x[0]);  // quiets a signaling NaN once
-                    }
-                } else {
-#pragma unroll
-                    for (int u = 0; u < U; ++u) acc = BinOp<OP, CD>::apply(acc, x[u]);
-                }
+                // float add: plain adds, replayed with the engine's NaN
+                // rule when the block's sum turns NaN; float max/min: an
+                // integer max/min of order keys when the block has no NaN
+                col_fold_batch<OP, CD, U>(acc, x);
             }
             for (; j < rn_in; ++j) {
                 T x;
@@ -589,38 +625,15 @@ __global__ void __launch_bounds__(RED_THREADS) k_red_col(RedDesc d) {
     }
 }
 
-// One batch of a column fold in order: float add sums plainly and replays
-// the batch with the engine's NaN rule only when the sum turns NaN (once the
-// accumulator is a quiet NaN no later add changes it).
-template <int OP, int CD, int U>
-__device__ __forceinline__ void col_fold_batch(typename DT<CD>::T& acc, const typename DT<CD>::T (&x)[U]) {
-    typedef typename DT<CD>::T T;
-    if constexpr (OP == OP_ADD && (CD == DT_F32 || CD == DT_F64)) {
-        if (acc == acc) {
-            T r = acc;
-#pragma unroll
-            for (int u = 0; u < U; ++u) r = plain_sum(r, x[u]);
-            if (r != r) {
-                r = acc;
-#pragma unroll
-                for (int u = 0; u < U; ++u) r = BinOp<OP, CD>::apply(r, x[u]);
-            }
-            acc = r;
-        } else {
-            acc = BinOp<OP, CD>::apply(acc, x[0]);  // quiets a signaling NaN once
-        }
-    } else {
-#pragma unroll
-        for (int u = 0; u < U; ++u) acc = BinOp<OP, CD>::apply(acc, x[u]);
-    }
-}
-
 // COL kernel, pipelined: one narrow axis, input in the loop dtype, too few
 // outputs for one batch of loads per thread to keep HBM busy. One thread per
 // output folds its column in order; its loads come in batches of U held in
 // two register buffers, the next batch issued before the current one is
 // folded, so U to 2U loads stay in flight per thread through the fold.
-constexpr int COLP_THREADS = 128;
+// One-warp CTAs, so the warps spread evenly over the SMs (32768 outputs are
+// 1024 warps: 6 or 7 per SM, where 128-thread CTAs put 4 on some SMs and 8
+// on others).
+constexpr int COLP_THREADS = 32;
 template <int OP, int CD, int U>
 __global__ void __launch_bounds__(COLP_THREADS) k_red_col_pipe(RedDesc d) {
     typedef typename DT<CD>::T T;
@@ -692,18 +705,15 @@ __global__ void __launch_bounds__(RED_THREADS) k_red_col_split(RedDesc d) {
                 const T* q = p + (j + (b + 1) * U) * rs;
 #pragma unroll
                 for (int u = 0; u < U; ++u) xb[u] = q[u * rs];
-#pragma unroll
-                for (int u = 0; u < U; ++u) acc = BinOp<OP, CD>::apply(acc, xa[u]);
+                col_fold_batch<OP, CD, U>(acc, xa);
                 if (b + 2 < nb) {
 #pragma unroll
                     for (int u = 0; u < U; ++u) xa[u] = q[(U + u) * rs];
                 }
-#pragma unroll
-                for (int u = 0; u < U; ++u) acc = BinOp<OP, CD>::apply(acc, xb[u]);
+                col_fold_batch<OP, CD, U>(acc, xb);
             }
             if (b < nb) {
-#pragma unroll
-                for (int u = 0; u < U; ++u) acc = BinOp<OP, CD>::apply(acc, xa[u]);
+                col_fold_batch<OP, CD, U>(acc, xa);
             }
         }
         for (int64_t k = j + nb * U; k < r1; ++k) acc = BinOp<OP, CD>::apply(acc, p[k * rs]);

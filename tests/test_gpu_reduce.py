@@ -323,6 +323,43 @@ def test_axis0_float_add_nan_payloads(shape, dt):
     check_reduce("add", a, d, axis=0, keepdims=True)
 
 
+@pytest.mark.parametrize("case", [((300, 4740), np.float32, None), ((257, 40000), np.float32, None),
+                                  ((260, 5000), np.float64, None), ((256, 20000), np.float64, None),
+                                  ((300, 6000), np.float32, (16, 4816)), ((300, 6000), np.float32, (1, 4801)),
+                                  ((290, 9000), np.int32, None), ((270, 5000), np.int64, None)], ids=str)
+def test_axis0_many_columns(case):
+    """Column folds over thousands of columns: a ragged last warp of
+    columns, row counts that are not a multiple of any batch, columns past
+    the 8 x 148 warps of one wave, a column slice whose rows are longer than
+    the kept extent and an unaligned one; each op in row order, with NaN
+    payloads, signaling NaNs, infinities and signed zeros for the floats
+    (float max/min fold NaN-free batches through integer order keys)."""
+    shape, dt, cols = case
+    rng = np.random.default_rng(shape[0] * 7 + shape[1])
+    if np.dtype(dt).kind == "f":
+        a = (rng.standard_normal(shape) * 3).astype(dt)
+        a = _nan_payloads(a, rng, 2e-4)
+        ib = np.uint32 if dt == np.float32 else np.uint64
+        a[0, ::17] = np.array([0x7FA00001 if dt == np.float32 else 0x7FF4000000000001], ib).view(dt)[0]
+        a[7, 2::19] = np.inf
+        a[11, 2::19] = -np.inf
+        a.reshape(-1)[rng.random(a.size) < 0.01] = -0.0
+        ops = ("add", "maximum", "minimum", "multiply", "subtract")
+    else:
+        a = rng.integers(-1000, 1000, shape).astype(dt)
+        ops = ("add", "multiply", "maximum", "bitwise_xor", "subtract")
+    base = ap.from_numpy(a)
+    if cols is not None:
+        a = a[:, cols[0]:cols[1]]
+        d = base[:, cols[0]:cols[1]]
+    else:
+        d = base
+    for op in ops:
+        check_reduce(op, a, d, axis=0)
+    check_reduce("add", a, d, axis=0, initial=a.dtype.type(2))
+    check_reduce("maximum", a, d, axis=0, keepdims=True)
+
+
 @pytest.mark.parametrize("shape,axis", [((64, 4096), 1), ((9, 32768), -1), ((3, 1 << 20), 1), ((1 << 22,), None),
                                         ((2, 16, 8192), (1, 2)), ((5, 65536), None)])
 def test_float32_power_of_two_runs(shape, axis):
