@@ -53,10 +53,35 @@ __host__ __device__ constexpr bool ew_prefetch_op(int op, int cd) {
     return (op == OP_FLOOR_DIVIDE || op == OP_REMAINDER || op == OP_FMOD) && (cd == DT_I32 || cd == DT_U32);
 }
 
+// N results of one vector of pairs. Ops with a branch-free fast path
+// (BinOp::FAST) evaluate the whole vector that way and redo it with apply()
+// and the FPE detector only when some pair lies outside the fast path, whose
+// pairs raise no FPE flag; the others apply() and detect per pair. Used by
+// the transposed tile kernel k_bin_trv1, where gathering a vector's pairs
+// before the arithmetic measured 4-10 % faster on the int32 / int64 /
+// float32 division family (float64 division keeps its per-pair loop there:
+// 5-10 % slower this way).
+template <int OP, int CD, bool FPE, int N>
+__device__ __forceinline__ void bin_vec(const typename DT<CD>::T (&x)[N], const typename DT<CD>::T (&y)[N],
+                                        typename BinOp<OP, CD>::R (&r)[N], uint32_t& bits) {
+    typedef BinOp<OP, CD> Op;
+    if constexpr (Op::FAST) {
+        bool ok = true;
+#pragma unroll
+        for (int k = 0; k < N; ++k) ok &= Op::fast(x[k], y[k], &r[k]);
+        if (ok) return;
+    }
+#pragma unroll
+    for (int k = 0; k < N; ++k) {
+        r[k] = Op::apply(x[k], y[k]);
+        if constexpr (FPE) bits |= fpe_bits<OP, CD>(x[k], y[k], r[k]);
+    }
+}
+
 template <int OP, int CD, bool FPE>
-__global__ void __launch_bounds__(EW_THREADS)
-k_bin_contig(const typename DT<CD>::T* __restrict__ a, const typename DT<CD>::T* __restrict__ b,
-             typename BinOp<OP, CD>::R* __restrict__ o, int64_t n, int a_sc, int b_sc, uint32_t* flags) {
+__device__ __forceinline__ void bin_contig_body(const typename DT<CD>::T* __restrict__ a, const typename DT<CD>::T* __restrict__ b,
+                                                typename BinOp<OP, CD>::R* __restrict__ o, int64_t n, int a_sc, int b_sc,
+                                                uint32_t* flags) {
     typedef typename DT<CD>::T T;
     typedef typename BinOp<OP, CD>::R R;
     constexpr int N = Vec16<T>::N;
@@ -129,6 +154,21 @@ k_bin_contig(const typename DT<CD>::T* __restrict__ a, const typename DT<CD>::T*
         o[i] = r;
     }
     if constexpr (FPE) flush_flags(bits, flags);
+}
+template <int OP, int CD, bool FPE>
+__global__ void __launch_bounds__(EW_THREADS)
+k_bin_contig(const typename DT<CD>::T* __restrict__ a, const typename DT<CD>::T* __restrict__ b,
+             typename BinOp<OP, CD>::R* __restrict__ o, int64_t n, int a_sc, int b_sc, uint32_t* flags) {
+    bin_contig_body<OP, CD, FPE>(a, b, o, n, a_sc, b_sc, flags);
+}
+// the same with three resident CTAs, for float64 floor_divide (80 registers,
+// 90 unbounded): measured 13 % faster, where the same bound made float64
+// remainder 14 % slower
+template <int OP, int CD, bool FPE>
+__global__ void __launch_bounds__(EW_THREADS, 3)
+k_bin_contig3(const typename DT<CD>::T* __restrict__ a, const typename DT<CD>::T* __restrict__ b,
+              typename BinOp<OP, CD>::R* __restrict__ o, int64_t n, int a_sc, int b_sc, uint32_t* flags) {
+    bin_contig_body<OP, CD, FPE>(a, b, o, n, a_sc, b_sc, flags);
 }
 
 // Offsets of flat index i over the merged dims (C order, last dim fastest).
@@ -450,13 +490,27 @@ k_bin_trv1(EwDesc d, uint32_t* flags) {
         for (int k = 0; k < V::PASS; ++k) {
             const int m = line + k * LSTEP;
             R r[V::VW];
+            if constexpr (sizeof(T) == 8 && Op::FAST) {
+                // float64 division: one pair at a time (measured faster
+                // here than gathering the vector first)
 #pragma unroll
-            for (int e = 0; e < V::VW; ++e) {
-                const T vt = ocol ? st[lane_v + e][m] : st[m][lane_v + e];
-                const T vd = xd[k].v[e];
-                const T x = swap ? vd : vt, y = swap ? vt : vd;
-                r[e] = Op::apply(x, y);
-                if constexpr (FPE) bits |= fpe_bits<OP, CD>(x, y, r[e]);
+                for (int e = 0; e < V::VW; ++e) {
+                    const T vt = ocol ? st[lane_v + e][m] : st[m][lane_v + e];
+                    const T vd = xd[k].v[e];
+                    const T x = swap ? vd : vt, y = swap ? vt : vd;
+                    r[e] = Op::apply(x, y);
+                    if constexpr (FPE) bits |= fpe_bits<OP, CD>(x, y, r[e]);
+                }
+            } else {
+                T xs[V::VW], ys[V::VW];
+#pragma unroll
+                for (int e = 0; e < V::VW; ++e) {
+                    const T vt = ocol ? st[lane_v + e][m] : st[m][lane_v + e];
+                    const T vd = xd[k].v[e];
+                    xs[e] = swap ? vd : vt;
+                    ys[e] = swap ? vt : vd;
+                }
+                bin_vec<OP, CD, FPE, V::VW>(xs, ys, r, bits);
             }
             R* dst = ocol ? po + (i0 + lane_v) + (j0 + m) * d.so[1] : po + (i0 + m) * d.so[0] + (j0 + lane_v);
             stv<R, V::VW>(dst, 0, r);

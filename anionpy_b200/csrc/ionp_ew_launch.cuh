@@ -47,10 +47,13 @@ cudaError_t launch_bin_t(const EwDesc& d, const ContigInfo& ci, uint32_t* flags,
         const T* a = (const T*)d.a.p;
         const T* b = (const T*)d.b.p;
         R* o = (R*)d.o;
-        if constexpr (HAS_FPE) {
-            if (fpe) { k_bin_contig<OP, CD, true><<<g, EW_THREADS, 0, s>>>(a, b, o, d.n, ci.a_scalar, ci.b_scalar, flags); count_launch(); return cudaGetLastError(); }
+        if constexpr (OP == OP_FLOOR_DIVIDE && CD == DT_F64) {
+            if (fpe) k_bin_contig3<OP, CD, true><<<g, EW_THREADS, 0, s>>>(a, b, o, d.n, ci.a_scalar, ci.b_scalar, flags);
+            else k_bin_contig3<OP, CD, false><<<g, EW_THREADS, 0, s>>>(a, b, o, d.n, ci.a_scalar, ci.b_scalar, flags);
+        } else {
+            if (HAS_FPE && fpe) k_bin_contig<OP, CD, HAS_FPE><<<g, EW_THREADS, 0, s>>>(a, b, o, d.n, ci.a_scalar, ci.b_scalar, flags);
+            else k_bin_contig<OP, CD, false><<<g, EW_THREADS, 0, s>>>(a, b, o, d.n, ci.a_scalar, ci.b_scalar, flags);
         }
-        k_bin_contig<OP, CD, false><<<g, EW_THREADS, 0, s>>>(a, b, o, d.n, ci.a_scalar, ci.b_scalar, flags);
         count_launch();
         return cudaGetLastError();
     }

@@ -171,12 +171,16 @@ template <class F> static __device__ __noinline__ F x_fmod_slow(F x, F y) {
     }
     return x;  // y infinite, x finite
 }
-template <class F> __device__ __forceinline__ F x_fmod(F x, F y) {
+template <class F> __device__ __forceinline__ bool fmod_fast(F x, F y, F* r) {
     F t, m;
-    if (quot_fast(x, y, &t, &m)) {
-        const F r = (m != (F)0 && signbit(m) != signbit(x)) ? m + copysign(y, x) : m;
-        return r == (F)0 ? copysign((F)0, x) : r;
-    }
+    const bool ok = quot_fast(x, y, &t, &m);
+    const F v = (m != (F)0 && signbit(m) != signbit(x)) ? m + copysign(y, x) : m;
+    *r = v == (F)0 ? copysign((F)0, x) : v;
+    return ok;
+}
+template <class F> __device__ __forceinline__ F x_fmod(F x, F y) {
+    F r;
+    if (fmod_fast(x, y, &r)) return r;
     return x_fmod_slow(x, y);
 }
 
@@ -495,15 +499,19 @@ template <int D> static __device__ __noinline__ typename FOps<D>::T floor_divide
 // other two cases (t exact, or one too large in magnitude below a negative
 // quotient with a nonzero remainder) it is t. A zero result takes the sign
 // of x XOR y. Everything else goes out of line.
+template <class T> __device__ __forceinline__ bool floor_divide_fast(T x, T y, T* r) {
+    T t, m;
+    const bool ok = quot_fast(x, y, &t, &m);
+    const T f = (m != (T)0 && signbit(m) != signbit(y)) ? t - (T)1 : t;
+    if constexpr (sizeof(T) == 4) *r = f == 0.0f ? bf((fb(x) ^ fb(y)) & 0x80000000u) : f;
+    else *r = f == 0.0 ? bd((db(x) ^ db(y)) & 0x8000000000000000ull) : f;
+    return ok;
+}
 template <int D> __device__ __forceinline__ typename FOps<D>::T float_floor_divide(typename FOps<D>::T x, typename FOps<D>::T y) {
     typedef typename FOps<D>::T T;
     if constexpr (D == DT_F32 || D == DT_F64) {
-        T t, m;
-        if (quot_fast(x, y, &t, &m)) {
-            const T f = (m != (T)0 && signbit(m) != signbit(y)) ? t - (T)1 : t;
-            if constexpr (D == DT_F32) return f == 0.0f ? bf((fb(x) ^ fb(y)) & 0x80000000u) : f;
-            else return f == 0.0 ? bd((db(x) ^ db(y)) & 0x8000000000000000ull) : f;
-        }
+        T r;
+        if (floor_divide_fast(x, y, &r)) return r;
         return floor_divide_slow<D>(x, y);
     }
     return floor_divide_full<D>(x, y);
@@ -541,6 +549,14 @@ template <class F> __device__ __forceinline__ F float_remainder(F x, F y) {
     if (r == (F)0) return copysign((F)0, y);
     if ((r < (F)0) != (y < (F)0)) return x_add(r, y);
     return r;
+}
+// its fast path (fmod_fast's pairs: r and y finite, so the add needs no NaN
+// rule)
+template <class F> __device__ __forceinline__ bool remainder_fast(F x, F y, F* r) {
+    F m;
+    const bool ok = fmod_fast(x, y, &m);
+    *r = m == (F)0 ? copysign((F)0, y) : (((m < (F)0) != (y < (F)0)) ? m + y : m);
+    return ok;
 }
 
 // ---------------------------------------------------------------------------
@@ -639,6 +655,16 @@ template <int OP, int CD> struct BinOp {
     typedef typename DT<CD>::T T;
     static constexpr int OUT_DT = (op_is_compare(OP) || op_is_logical(OP)) ? DT_BOOL : CD;
     typedef typename DT<OUT_DT>::T R;
+    // float floor_divide / remainder / fmod: fast(x, y, &r) is true, with r
+    // = apply(x, y), for the pairs of their branch-free fast path, and
+    // those pairs raise no FPE flag (the divisor is nonzero)
+    static constexpr bool FAST = (CD == DT_F32 || CD == DT_F64) &&
+                                 (OP == OP_FLOOR_DIVIDE || OP == OP_REMAINDER || OP == OP_FMOD);
+    static __device__ __forceinline__ bool fast(T x, T y, R* r) {
+        if constexpr (OP == OP_FLOOR_DIVIDE) return floor_divide_fast(x, y, r);
+        else if constexpr (OP == OP_REMAINDER) return remainder_fast(x, y, r);
+        else return fmod_fast(x, y, r);
+    }
     static __device__ __forceinline__ R apply(T x, T y) {
         if constexpr (op_is_compare(OP)) {
             if constexpr (CD == DT_F16) return cmp(h2f(x), h2f(y));

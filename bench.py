@@ -800,9 +800,16 @@ def main():
 # still held in L2 when a launch ends are not counted, so the full-size
 # ratio approaches 1.0). sin/float64/step2 at 2^24 elements: 268.5 MB read
 # (a step-2 slice reads every other 8-byte element, so whole sectors are
-# twice the logical bytes) + 78.1 MB written of 268.4 MB.
+# twice the logical bytes) + 78.1 MB written of 268.4 MB. At 40,960,000
+# elements (983 MB algorithmic for an int64 / float64 binary): the step-2
+# division cases read 1310.7-1310.8 MB (both operands twice) and write
+# 272.6-276.6 MB, the transposed int64 ones read 655.4 MB and write
+# 290.2-294.2 MB.
 NCU_TRAFFIC_PER_BYTE = {"floor_divide/float64/transposed": 0.9800, "add/float32/contig": 0.9536,
-                        "sin/float64/step2": 1.2913}
+                        "sin/float64/step2": 1.2913,
+                        "remainder/int64/step2": 1.6114, "floor_divide/int64/step2": 1.6111,
+                        "floor_divide/float64/step2": 1.6148, "remainder/int64/transposed": 0.9653,
+                        "floor_divide/int64/transposed": 0.9660}
 
 
 def traffic_of(case, alg_bytes):
