@@ -162,24 +162,31 @@ LM_FN float log32(float x) {
 // n and the remainder from 96 bits of 2/pi in integer arithmetic. The
 // quadrant picks the sin or cos polynomial and its sign. (s_sinf.c,
 // sincosf.h)
-// sin (n even) or cos (n odd) polynomial of the reduced argument; both are
-// evaluated and one selected, so lanes of a warp in different quadrants run
-// one body. flip negates the cos polynomial (the table's second half).
+// sin (n even) or cos (n odd) polynomial of the reduced argument, in the
+// operation order of each:
+//   sin: fma(x7, fma(x2, S3, S2), fma(x3, S1, x)),  x3 = x x2, x7 = x3 x2
+//   cos: fma(x6, fma(x2, C4, C3), fma(x4, C2, fma(x2, C1, C0))),
+//        x4 = x2 x2, x6 = x4 x2
+// Both have the same shape -- p = fma(x2, A, B), u = y x2, w = u x2,
+// fma(w, p, fma(u, K, L)) -- so one body evaluates whichever the lane needs
+// with its own coefficients, the same operations on the same operands as
+// the polynomial alone (lanes of a warp in different quadrants still run
+// one body). flip negates the cos coefficients (the table's second half),
+// which is exact.
 LM_FN float sin32_poly(double x, double x2, int n, bool flip) {
     const double S1 = -0x1.555545995a603p-3, S2 = 0x1.1107605230bc4p-7, S3 = -0x1.994eb3774cf24p-13;
-    const double x3 = x * x2;
-    const double s1 = fmad(x2, S3, S2);
-    const double x7 = x3 * x2;
-    const double sp = fmad(x7, s1, fmad(x3, S1, x));
-    const double sg = flip ? -1.0 : 1.0;
-    const double C0 = sg * 0x1p0, C1 = sg * -0x1.ffffffd0c621cp-2, C2 = sg * 0x1.55553e1068f19p-5,
-                 C3 = sg * -0x1.6c087e89a359dp-10, C4 = sg * 0x1.99343027bf8c3p-16;
-    const double x4 = x2 * x2;
-    const double c2 = fmad(x2, C4, C3);
-    const double c1 = fmad(x2, C1, C0);
-    const double x6 = x4 * x2;
-    const double cp = fmad(x6, c2, fmad(x4, C2, c1));
-    return (float)((n & 1) ? cp : sp);
+    const double C0 = 0x1p0, C1 = -0x1.ffffffd0c621cp-2, C2 = 0x1.55553e1068f19p-5,
+                 C3 = -0x1.6c087e89a359dp-10, C4 = 0x1.99343027bf8c3p-16;
+    const bool c = (n & 1) != 0;
+    const double A = c ? (flip ? -C4 : C4) : S3;
+    const double B = c ? (flip ? -C3 : C3) : S2;
+    const double K = c ? (flip ? -C2 : C2) : S1;
+    const double p = fmad(x2, A, B);                 // s1 / c2
+    const double u = (c ? x2 : x) * x2;              // x3 / x4
+    const double w = u * x2;                          // x7 / x6
+    const double c1 = fmad(x2, flip ? -C1 : C1, flip ? -C0 : C0);
+    const double v = fmad(u, K, c ? c1 : x);
+    return (float)fmad(w, p, v);
 }
 LM_SLOW double sin32_reduce_large(uint32_t xi, int* np) {
     const unsigned int* w = &TWO_OVER_PI_W[(xi >> 26) & 15];
