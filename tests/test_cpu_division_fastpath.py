@@ -1,0 +1,144 @@
+"""CPU check of the arithmetic behind the GPU division fast path (`quot_fast`,
+`floor_divide_fast`, `fmod_fast` in anionpy_b200/csrc/ionp_scalar.cuh),
+with exact rational arithmetic as the judge of every claim.
+
+The hardware reciprocal approximation is modelled by every float32 value
+within 1 ulp of the exact reciprocal (its documented bound), so each pair is
+checked for all the reciprocals the hardware may return. For every pair the
+fast path accepts:
+  * t = trunc(p) is the truncated quotient q or q + 1 in magnitude;
+  * m = x - t*y is a representable value (one fused multiply-add is exact);
+  * t - [m != 0 and sign(m) != sign(y)] is the exact floor of x / y;
+  * m, with y added back (x's sign) when m has the sign opposite to x's, is
+    the exact fmod of x and y.
+Pairs: quotients a rounding away from integers at every scale up to the
+fast path's limit (2^19 float32, 2^36 float64), divisors over the whole
+accepted range 2^-125 ... 2^125, subnormal dividends."""
+import math
+from fractions import Fraction
+
+import numpy as np
+
+F32_MAX_Q = 2.0 ** 19
+F64_MAX_Q = 2.0 ** 36
+
+
+def rn32(fr):
+    """a Fraction rounded to the nearest value with 24 significant bits (ties
+    to even), as a float32: float32 rounding in the normal range (the
+    subnormal dividends' products lie far below 1, where the fast path's
+    outcome does not depend on their last bits)"""
+    return np.float32(_rn_bits(fr, 24))
+
+
+def rn64(fr):
+    return _rn_bits(fr, 53)
+
+
+def _rn_bits(fr, bits):
+    """nearest binary float with `bits` significant bits (normal range,
+    ties to even), as a Python float (exact for bits <= 53)"""
+    if fr == 0:
+        return 0.0
+    s = -1 if fr < 0 else 1
+    a = abs(fr)
+    e = a.numerator.bit_length() - a.denominator.bit_length()
+    if Fraction(2) ** e > a:
+        e -= 1
+    # a in [2^e, 2^(e+1)); scale the significand to an integer of `bits` bits
+    sc = Fraction(2) ** (bits - 1 - e)
+    v = a * sc
+    n = v.numerator // v.denominator
+    rem = v - n
+    if rem > Fraction(1, 2) or (rem == Fraction(1, 2) and n % 2 == 1):
+        n += 1
+    return s * float(Fraction(n) / sc)
+
+
+def rcp32_candidates(yf):
+    """every float32 within 1 ulp of 1/yf (yf a float32, normal reciprocal)"""
+    exact = 1 / Fraction(float(yf))
+    r = rn32(exact)
+    out = []
+    for c in (np.nextafter(r, np.float32(-np.inf)), r, np.nextafter(r, np.float32(np.inf))):
+        ulp = Fraction(float(np.spacing(np.float32(abs(c)))))
+        if abs(Fraction(float(c)) - exact) <= ulp:
+            out.append(c)
+    return out
+
+
+def check_pair(x, y, t, m_exact):
+    """the four claims for one accepted pair (x, y, t as Fractions)"""
+    q_exact = x / y
+    q_trunc = Fraction(math.trunc(q_exact))
+    assert abs(t) in (abs(q_trunc), abs(q_trunc) + 1), (x, y, t)
+    # floor
+    dec = m_exact != 0 and (m_exact < 0) != (y < 0)
+    assert t - (1 if dec else 0) == math.floor(q_exact), (x, y, t)
+    # fmod
+    fm = m_exact
+    if fm != 0 and (fm < 0) != (x < 0):
+        fm = fm + (abs(y) if x > 0 else -abs(y))
+    assert fm == x - q_trunc * y, (x, y, t)
+
+
+def pairs(rng, n, qmax, emin, emax, dt):
+    """seeded pairs: y over the accepted exponent range, quotients near
+    integers of every scale up to qmax, both signs"""
+    e = rng.integers(emin, emax + 1, n)
+    y = rng.uniform(1.0, 2.0, n) * np.exp2(e.astype(np.float64)) * rng.choice([-1.0, 1.0], n)
+    y = y.astype(dt)
+    scale = np.exp2(rng.uniform(-3, math.log2(qmax), n))
+    q = np.round(scale) + rng.choice([-1e-7, 0.0, 1e-7, 0.3, 0.5, 0.999], n) * (dt == np.float32) \
+        + rng.choice([-1e-15, 0.0, 1e-15, 0.3, 0.5, 0.999], n) * (dt == np.float64)
+    with np.errstate(over="ignore"):  # an infinite dividend is skipped by the caller
+        x = (q * y.astype(np.float64) * rng.choice([-1.0, 1.0], n)).astype(dt)
+    return x, y
+
+
+def test_float32_fast_path_claims():
+    rng = np.random.default_rng(20261204)
+    x, y = pairs(rng, 6000, F32_MAX_Q, -125, 124, np.float32)
+    # subnormal dividends over small divisors
+    xs = (rng.uniform(-1, 1, 200) * 2.0 ** -128).astype(np.float32)
+    ys = (rng.uniform(1, 2, 200) * np.exp2(rng.integers(-125, -100, 200).astype(np.float64))).astype(np.float32)
+    x, y = np.concatenate([x, xs]), np.concatenate([y, ys])
+    checked = 0
+    for xf, yf in zip(x, y):
+        if not (np.isfinite(xf) and 2.0 ** -125 <= abs(float(yf)) <= 2.0 ** 125):
+            continue
+        X, Y = Fraction(float(xf)), Fraction(float(yf))
+        for rc in rcp32_candidates(yf):
+            p = rn32(Fraction(float(rn32(X * Fraction(float(rc))))) * (1 + Fraction(1, 2 ** 20)))
+            if not abs(float(p)) < F32_MAX_Q:
+                continue
+            t = Fraction(math.trunc(float(p)))
+            m = X - t * Y
+            assert Fraction(float(rn32(m))) == m, (xf, yf, t)  # one FMA is exact
+            check_pair(X, Y, t, m)
+            checked += 1
+    assert checked >= 6000  # at least one modelled reciprocal per pair
+
+
+def test_float64_fast_path_claims():
+    rng = np.random.default_rng(20261205)
+    x, y = pairs(rng, 4000, F64_MAX_Q, -125, 124, np.float64)
+    checked = 0
+    for xd, yd in zip(x, y):
+        if not (np.isfinite(xd) and 2.0 ** -125 <= abs(float(yd)) <= 2.0 ** 125):
+            continue
+        X, Y = Fraction(float(xd)), Fraction(float(yd))
+        yf = np.float32(yd)  # the float32 the reciprocal approximation sees
+        for rc in rcp32_candidates(yf):
+            r0 = Fraction(float(rc))
+            e = Fraction(rn64(1 - Y * r0))           # fma(-y, r0, 1)
+            r1 = Fraction(rn64(r0 + r0 * e))         # fma(r0, e, r0)
+            p = rn64(Fraction(rn64(X * r1)) * (1 + Fraction(1, 2 ** 38)))
+            if not abs(p) < F64_MAX_Q:
+                continue
+            t = Fraction(math.trunc(p))
+            m = X - t * Y
+            assert Fraction(rn64(m)) == m, (xd, yd, t)  # one FMA is exact
+            check_pair(X, Y, t, m)
+            checked += 1
+    assert checked >= 4000  # at least one modelled reciprocal per pair
