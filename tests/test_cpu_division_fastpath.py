@@ -1,6 +1,7 @@
-"""CPU check of the arithmetic behind the GPU division fast path (`quot_fast`,
-`floor_divide_fast`, `fmod_fast` in anionpy_b200/csrc/ionp_scalar.cuh),
-with exact rational arithmetic as the judge of every claim.
+"""CPU check of the arithmetic behind the GPU division fast paths (`quot_fast`,
+`floor_divide_fast`, `fmod_fast` and `udiv64_trunc` in
+anionpy_b200/csrc/ionp_scalar.cuh), with exact rational arithmetic as the
+judge of every claim.
 
 The hardware reciprocal approximation is modelled by every float32 value
 within 1 ulp of the exact reciprocal (its documented bound), so each pair is
@@ -142,3 +143,59 @@ def test_float64_fast_path_claims():
             check_pair(X, Y, t, m)
             checked += 1
     assert checked >= 4000  # at least one modelled reciprocal per pair
+
+
+def _f32_rz(u):
+    """a non-negative integer rounded toward zero to float32 (24 bits)"""
+    if u < (1 << 24):
+        return Fraction(u)
+    sh = u.bit_length() - 24
+    return Fraction((u >> sh) << sh)
+
+
+def _f32_ru(u):
+    """a positive integer rounded up to float32 (24 bits)"""
+    if u < (1 << 24):
+        return Fraction(u)
+    sh = u.bit_length() - 24
+    top = u >> sh
+    if (top << sh) != u:
+        top += 1
+    return Fraction(top << sh)
+
+
+def test_int64_quotient_estimate_claims():
+    """`udiv64_trunc`: fq = rn(rn(rz(ux) * rcp(ru(uy))) * (1 - 2^-20)) stays
+    below ux / uy, so q = trunc(fq) never overshoots (ux - q uy cannot wrap),
+    and below 2^20 it is at most two below the true quotient, which the two
+    remainder steps repair; for every float32 reciprocal within 1 ulp."""
+    rng = np.random.default_rng(20261206)
+    cases = []
+    for _ in range(3000):
+        kind = rng.integers(0, 4)
+        uy = int(rng.integers(1, 1 << int(rng.integers(1, 63))))
+        if kind == 0:    # near-multiples
+            q = int(rng.integers(1, 1 << 20))
+            ux = q * uy + int(rng.integers(-2, 3))
+        elif kind == 1:  # quotients near the 2^20 limit
+            ux = ((1 << 20) + int(rng.integers(-4, 4))) * uy + int(rng.integers(0, uy))
+        elif kind == 2:  # powers of two
+            uy = 1 << int(rng.integers(0, 40))
+            ux = int(rng.integers(0, 1 << 62))
+        else:            # random bits
+            ux = int(rng.integers(0, 1 << 63))
+        if 0 < ux < (1 << 64) and uy > 0 and ux >= uy:
+            cases.append((ux, uy))
+    checked = 0
+    for ux, uy in cases:
+        yr = float(_f32_ru(uy))
+        for rc in rcp32_candidates(np.float32(yr)):
+            fq = rn32(Fraction(float(rn32(_f32_rz(ux) * Fraction(float(rc))))) * (1 - Fraction(1, 2 ** 20)))
+            if not float(fq) < 2.0 ** 20:
+                continue
+            q_est = math.trunc(float(fq))
+            q = ux // uy
+            assert q_est <= q, (ux, uy)          # ux - q_est uy does not wrap
+            assert q - q_est <= 2, (ux, uy)      # two repairs suffice
+            checked += 1
+    assert checked >= 1000
