@@ -199,3 +199,51 @@ def test_int64_quotient_estimate_claims():
             assert q - q_est <= 2, (ux, uy)      # two repairs suffice
             checked += 1
     assert checked >= 1000
+
+
+def _fast_results(x, y, dt):
+    """floor_divide / fmod / remainder of the fast path's formulas (the
+    reciprocal taken correctly rounded, one of the values the hardware
+    approximation may return), and the mask of pairs the fast path takes"""
+    one = dt(1)
+    if dt == np.float32:
+        rc = one / y
+        p = (x * rc) * np.float32(1 + 2.0 ** -20)
+        lim, lo, hi = 2.0 ** 19, 2.0 ** -125, 2.0 ** 125
+    else:
+        rc = one / y
+        p = (x * rc) * (1 + 2.0 ** -38)
+        lim, lo, hi = 2.0 ** 36, 2.0 ** -125, 2.0 ** 125
+    ok = np.isfinite(x) & (np.abs(y) >= lo) & (np.abs(y) <= hi) & (np.abs(p) < lim)
+    t = np.trunc(np.where(ok, p, 0)).astype(dt)
+    # m = x - t y is exact (test_*_fast_path_claims); computed exactly here
+    m = np.array([float(Fraction(float(a)) - Fraction(float(b)) * Fraction(float(c)))
+                  for a, b, c in zip(np.where(ok, x, 0), t, np.where(ok, y, 1))]).astype(dt)
+    sx, sy, sm = np.signbit(x), np.signbit(y), np.signbit(m)
+    f = np.where((m != 0) & (sm != sy), t - one, t)
+    zero_xy = np.where(sx != sy, dt(-0.0), dt(0.0))
+    fdiv = np.where(f == 0, zero_xy, f)
+    v = np.where((m != 0) & (sm != sx), m + np.copysign(y, x), m)
+    fmod = np.where(v == 0, np.copysign(dt(0.0), x), v)
+    rem = np.where(fmod == 0, np.copysign(dt(0.0), y),
+                   np.where((fmod < 0) != (y < 0), fmod + y, fmod))
+    return ok, {"floor_divide": fdiv, "fmod": fmod, "remainder": rem}
+
+
+def test_fast_path_results_match_the_oracle():
+    """The fast path's result formulas (zero signs included) against the
+    oracle's floor_divide / fmod / remainder, bit for bit, on the pairs the
+    fast path takes."""
+    from oracle import oracle as O
+    rng = np.random.default_rng(20261207)
+    for dt, qmax in ((np.float32, F32_MAX_Q), (np.float64, F64_MAX_Q)):
+        x, y = pairs(rng, 6000, qmax, -125, 124, dt)
+        x[:300] = rng.choice([0.0, -0.0], 300).astype(dt)            # signed zero dividends
+        x[300:600] = (y[300:600] * dt(0.25)) * rng.choice([-1, 1], 300).astype(dt)  # |x / y| < 1
+        ok, got = _fast_results(x, y, dt)
+        assert ok.sum() > 5000
+        ib = np.uint32 if dt == np.float32 else np.uint64
+        for op, r in got.items():
+            want, _ = O.binary(op, x, y)
+            bad = np.nonzero(ok & (r.view(ib) != np.asarray(want).view(ib)))[0]
+            assert bad.size == 0, (op, np.dtype(dt).name, x[bad[:3]], y[bad[:3]], r[bad[:3]], want[bad[:3]])
