@@ -30,6 +30,9 @@ def test_key_fold_matches_oracle(dt, op):
     a[rng.random(a.shape) < 0.3] = 0.0
     a[rng.random(a.shape) < 0.3] *= -1                            # -0 among the zeros
     a[:, :4] = rng.choice([0.0, -0.0], (300, 4)).astype(dt)      # columns of zeros only
+    a[:, 20:40] = -np.abs(a[:, 20:40]) - dt(0.5)                  # all negative
+    a[:, 40:60] = np.abs(a[:, 40:60]) + dt(0.5)                   # all positive
+    a[:, 60:64] = np.where(rng.random((300, 4)) < 0.5, dt(-0.0), dt(-1.0))  # -0 the largest
     a[5, 10] = np.inf
     a[7, 11] = -np.inf
     ib = np.uint32 if dt == np.float32 else np.uint64
