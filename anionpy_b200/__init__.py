@@ -12,7 +12,7 @@ from ._batch import Batch
 from ._fpstate import errstate, geterr, geterrcall, seterr, seterrcall
 from ._lib import AxisError, UFuncTypeError, launch_count
 from ._ufunc import (BINARY_OPS, UNARY_OPS, absolute, add, argmax, argmin, bitwise_and, bitwise_not, bitwise_or,
-                     bitwise_xor, divide, equal, exp, floor_divide, fmod, greater, greater_equal, invert, left_shift,
+                     bitwise_xor, cos, divide, equal, exp, floor_divide, fmod, greater, greater_equal, invert, left_shift,
                      less, less_equal, log, logical_and, logical_not, logical_or, logical_xor, maximum, minimum, mod,
                      multiply, negative, not_equal, remainder, right_shift, sin, sqrt, subtract, true_divide, ufunc)
 from ._ufunc import abs  # noqa: A001

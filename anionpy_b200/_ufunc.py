@@ -29,7 +29,7 @@ BINARY_OPS = {
 }
 UNARY_OPS = {
     "negative": 64, "absolute": 65, "invert": 66, "logical_not": 67,
-    "sqrt": 80, "exp": 81, "log": 82, "sin": 83,
+    "sqrt": 80, "exp": 81, "log": 82, "sin": 83, "cos": 84,
 }
 # ops that have a post-hoc FPE detector (lib.rs:9077-9138)
 _FPE_KIND = {"divide": "divide", "floor_divide": "divide", "remainder": "remainder", "fmod": "remainder",

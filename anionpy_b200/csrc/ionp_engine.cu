@@ -53,7 +53,7 @@ const char* op_name(int op) {
         case OP_REMAINDER: return "remainder"; case OP_FMOD: return "fmod";
         case OP_NEGATIVE: return "negative"; case OP_ABSOLUTE: return "absolute"; case OP_INVERT: return "invert";
         case OP_LOGICAL_NOT: return "logical_not"; case OP_SQRT: return "sqrt"; case OP_EXP: return "exp";
-        case OP_LOG: return "log"; case OP_SIN: return "sin";
+        case OP_LOG: return "log"; case OP_SIN: return "sin"; case OP_COS: return "cos";
     }
     return "?";
 }
@@ -148,7 +148,7 @@ int32_t unary_loop(int op, int a, int* cd, int* rd) {
             *cd = *rd = a;
             return IONP_OK;
         case OP_ABSOLUTE: *cd = *rd = a; return IONP_OK;
-        case OP_SQRT: case OP_EXP: case OP_LOG: case OP_SIN:
+        case OP_SQRT: case OP_EXP: case OP_LOG: case OP_SIN: case OP_COS:
             // math_unary_out_dtype float tiers (ufunc.rs:1705-1712)
             if (a == DT_BOOL || a == DT_I8 || a == DT_U8) *cd = DT_F16;
             else if (a == DT_I16 || a == DT_U16) *cd = DT_F32;

@@ -30,7 +30,7 @@ template <int OP, int CD> constexpr bool un_valid() {
     if (OP == OP_NEGATIVE) return CD != DT_BOOL;
     if (OP == OP_ABSOLUTE) return true;
     if (OP == OP_INVERT) return !dt_is_float(CD);
-    return dt_is_float(CD);  // sqrt / exp / log / sin
+    return dt_is_float(CD);  // sqrt / exp / log / sin / cos
 }
 
 template <int OP, int CD>
@@ -85,6 +85,7 @@ cudaError_t launch_unary(int op, int cd, const EwDesc& d, const ContigInfo& ci, 
         case OP_EXP: return launch_un_op<OP_EXP>(cd, d, ci, f, s);
         case OP_LOG: return launch_un_op<OP_LOG>(cd, d, ci, f, s);
         case OP_SIN: return launch_un_op<OP_SIN>(cd, d, ci, f, s);
+        case OP_COS: return launch_un_op<OP_COS>(cd, d, ci, f, s);
     }
     return cudaErrorInvalidValue;
 }

@@ -226,6 +226,35 @@ LM_FN float sin32(float y) {
     return top < 0x398 ? y : r;                // |y| < 2^-12: y itself
 }
 
+// ------------------------------------------------------------------ cos32
+// The same reductions and polynomials as sin32 (s_cosf.c, sincosf.h): below
+// pi/4 the cos polynomial (1 below 2^-12); above, quadrant n + 1 of the
+// reduced argument, the sign and table half from n (and the input's sign
+// for the large reduction, which works on |y|).
+LM_FN float cos32(float y) {
+    const uint32_t ux = fbits(y);
+    const uint32_t top = (ux >> 20) & 0x7ff;
+    if (top >= 0x42f) {                        // |y| >= 120, inf, NaN
+        if (top >= 0x7f8) return (ux & 0x7FFFFFu) ? quiet32(y) : dnan32();
+        int n;
+        const int sign = (int)(ux >> 31);
+        const double x = sin32_reduce_large(ux, &n);
+        const int q = n + sign;
+        const double s = ((q + 1) & 2) ? -1.0 : 1.0;   // signs {1,-1,-1,1}[q & 3]
+        return sin32_poly(x * s, x * x, n ^ 1, (q & 2) != 0);
+    }
+    double x = (double)y;
+    if (top < 0x3f4) {                         // |y| < pi/4
+        if (top < 0x398) return 1.0f;          // |y| < 2^-12
+        return sin32_poly(x, x * x, 1, false);
+    }
+    const double r = x * 0x1.45F306DC9C883p+23;       // x * 2/pi * 2^24
+    const int n = ((int32_t)r + 0x800000) >> 24;
+    x = fmad(-(double)n, 0x1.921FB54442D18p0, x);
+    const double s = ((n + 1) & 2) ? -1.0 : 1.0;
+    return sin32_poly(x * s, x * x, n ^ 1, (n & 2) != 0);
+}
+
 // ------------------------------------------------------------------ exp64
 // e^x = 2^(k/128) e^r, x = k ln2/128 + r; 2^(k/128) = H (1 + t) from the
 // table, e^r - 1 by a quintic; result scale + scale * tmp. Results near
@@ -467,6 +496,43 @@ LM_FN double sin64(double x) {
         const double xn = t - 0x1.8p52;
         const double y = fmad(-xn, LM_MP2, fmad(-xn, LM_MP1, x));
         n = (int)(dbits(t) & 3);
+        const double t2 = fmad(-xn, LM_PP3, y);
+        da = fmad(-xn, LM_PP3, y - t2);
+        a = fmad(-xn, LM_PP4, t2);
+        da += fmad(-xn, LM_PP4, t2 - a);
+    }
+    return sin64_quadrant(a, da, n);
+}
+
+// cos: 1 below 2^-27; do_cos below 0.855469; do_sin of pi/2 - |x| as a
+// normalised double-double below 2.426265; quadrant n + 1 of the Cody-Waite
+// or the large reduction above (s_sin.c's __cos).
+LM_SLOW double cos64_large(double x) {
+    double a, da;
+    const int n = sin64_reduce_large(x, &a, &da);
+    return sin64_quadrant(a, da, n + 1);
+}
+LM_FN double cos64(double x) {
+    const uint32_t k = (uint32_t)(dbits(x) >> 32) & 0x7fffffffu;
+    if (k < 0x3e400000u) return 1.0;                      // |x| < 2^-27
+    if (k >= 0x419921fbu) {                              // |x| >= 105414350, inf, NaN
+        if (k < 0x7ff00000u) return cos64_large(x);
+        return ((dbits(x) << 12) != 0) ? quiet64(x) : dnan64();
+    }
+    double a, da;
+    int n;
+    if (k < 0x3feb6000u) {                               // |x| < 0.855469: cos(x)
+        a = x; da = 0.0; n = 1;
+    } else if (k < 0x400368fdu) {                        // |x| < 2.426265: sin(pi/2 - |x|)
+        const double y = LM_HP0 - fabs(x);
+        a = y + LM_HP1;
+        da = (y - a) + LM_HP1;
+        n = 0;
+    } else {                                             // Cody-Waite: x - n pi/2 in four parts
+        const double t = fmad(x, 0x1.45f306dc9c883p-1, 0x1.8p52);   // x 2/pi + shifter
+        const double xn = t - 0x1.8p52;
+        const double y = fmad(-xn, LM_MP2, fmad(-xn, LM_MP1, x));
+        n = (int)(dbits(t) & 3) + 1;
         const double t2 = fmad(-xn, LM_PP3, y);
         da = fmad(-xn, LM_PP3, y - t2);
         a = fmad(-xn, LM_PP4, t2);

@@ -1,5 +1,5 @@
 // Unary op table (ufunc.rs:3824-3975 unary_op, 4237-4367 math_unary_f32/f64);
-// exp/log/sin are the C-library restatements of ionp_libm.cuh.
+// exp/log/sin/cos are the C-library restatements of ionp_libm.cuh.
 #pragma once
 #include "ionp_scalar.cuh"
 #include "ionp_libm.cuh"
@@ -30,13 +30,15 @@ template <int OP, int CD> struct UnOp {
         if constexpr (OP == OP_SQRT) return x_sqrt(x);
         else if constexpr (OP == OP_EXP) return lm::exp32(x);
         else if constexpr (OP == OP_LOG) return lm::log32(x);
-        else return lm::sin32(x);
+        else if constexpr (OP == OP_SIN) return lm::sin32(x);
+        else return lm::cos32(x);
     }
     static __device__ __forceinline__ double f64op(double x) {
         if constexpr (OP == OP_SQRT) return x_sqrt(x);
         else if constexpr (OP == OP_EXP) return lm::exp64(x);
         else if constexpr (OP == OP_LOG) return lm::log64(x);
-        else return lm::sin64(x);
+        else if constexpr (OP == OP_SIN) return lm::sin64(x);
+        else return lm::cos64(x);
     }
     // detect_sqrt / detect_log (fpe.rs:359-396): x < 0 -> invalid,
     // log(0) -> divide.

@@ -30,7 +30,7 @@ enum : int {
     OP_FLOOR_DIVIDE, OP_LEFT_SHIFT, OP_RIGHT_SHIFT,
     OP_REMAINDER = 32, OP_FMOD = 33,
     OP_NEGATIVE = 64, OP_ABSOLUTE = 65, OP_INVERT = 66, OP_LOGICAL_NOT = 67,
-    OP_SQRT = 80, OP_EXP = 81, OP_LOG = 82, OP_SIN = 83,
+    OP_SQRT = 80, OP_EXP = 81, OP_LOG = 82, OP_SIN = 83, OP_COS = 84,
 };
 
 // FPE category bits (ionp-core/src/fpe.rs:43-48)

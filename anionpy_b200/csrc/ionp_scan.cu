@@ -521,6 +521,7 @@ cudaError_t launch_at_unary(int op, int cd, const AtDesc& d, cudaStream_t s) {
         case OP_EXP: return at_un_op<OP_EXP>(cd, d, s);
         case OP_LOG: return at_un_op<OP_LOG>(cd, d, s);
         case OP_SIN: return at_un_op<OP_SIN>(cd, d, s);
+        case OP_COS: return at_un_op<OP_COS>(cd, d, s);
     }
     return cudaErrorInvalidValue;
 }
@@ -640,8 +641,8 @@ extern "C" int32_t ionp_at(int32_t op, IonpArr* target, const int64_t* indices, 
     if (values && (st = check_arr(values, "values"))) return st;
     if (nindices < 0 || (nindices > 0 && !indices)) return set_err(IONP_ERR_INVALID, "bad indices");
     cudaStream_t s = (cudaStream_t)stream;
-    const bool unary = op >= OP_NEGATIVE && op <= OP_SIN;
-    const bool math_un = op >= OP_SQRT && op <= OP_SIN;
+    const bool unary = op >= OP_NEGATIVE && op <= OP_COS;
+    const bool math_un = op >= OP_SQRT && op <= OP_COS;
     if (!unary && !(op >= OP_ADD && op <= OP_RIGHT_SHIFT) && op != OP_REMAINDER && op != OP_FMOD)
         return set_err(IONP_ERR_UNSUPPORTED, std::string("op ") + std::to_string(op) + " has no .at in this engine");
     if (unary && values) return set_err(IONP_ERR_INVALID, "unary ufunc .at() takes no third argument");

@@ -47,7 +47,7 @@ enum {
     IONP_FLOOR_DIVIDE, IONP_LEFT_SHIFT, IONP_RIGHT_SHIFT,
     IONP_REMAINDER = 32, IONP_FMOD = 33,
     IONP_NEGATIVE = 64, IONP_ABSOLUTE = 65, IONP_INVERT = 66, IONP_LOGICAL_NOT = 67,
-    IONP_SQRT = 80, IONP_EXP = 81, IONP_LOG = 82, IONP_SIN = 83
+    IONP_SQRT = 80, IONP_EXP = 81, IONP_LOG = 82, IONP_SIN = 83, IONP_COS = 84
 };
 
 /* status codes: 1:1 with IonpError variants (ionp-core/src/error.rs:8-40),

@@ -110,7 +110,7 @@ enum {
     OP_FLOOR_DIVIDE, OP_LEFT_SHIFT, OP_RIGHT_SHIFT,
     OP_REMAINDER = 32, OP_FMOD = 33,
     OP_NEGATIVE = 64, OP_ABSOLUTE = 65, OP_INVERT = 66, OP_LOGICAL_NOT = 67,
-    OP_SQRT = 80, OP_EXP = 81, OP_LOG = 82, OP_SIN = 83,
+    OP_SQRT = 80, OP_EXP = 81, OP_LOG = 82, OP_SIN = 83, OP_COS = 84,
 };
 
 // status codes
@@ -157,7 +157,7 @@ static int unary_out_dtype(int op, int a, int* out) {
         case OP_NEGATIVE: if (a == D_BOOL) return ST_TYPE; *out = a; return ST_OK;
         case OP_INVERT: if (kind_of(a) == K_FLOAT) return ST_TYPE; *out = a; return ST_OK;
         case OP_ABSOLUTE: *out = a; return ST_OK;
-        case OP_SQRT: case OP_EXP: case OP_LOG: case OP_SIN:
+        case OP_SQRT: case OP_EXP: case OP_LOG: case OP_SIN: case OP_COS:
             if (a == D_BOOL || a == D_I8 || a == D_U8) *out = D_F16;
             else if (a == D_I16 || a == D_U16) *out = D_F32;
             else if (kind_of(a) != K_FLOAT) *out = D_F64;
@@ -1341,12 +1341,13 @@ int oracle_unary(int op, const OrArr* a, OrArr* out, int* fpe) {
                     case D_F64: { uint64_t x = dbits(atc<double>(c, i)); ((uint64_t*)o)[i] = neg ? (x ^ 0x8000000000000000ull) : (x & 0x7FFFFFFFFFFFFFFFull); } break;
                 }
             } break;
-            case OP_SQRT: case OP_EXP: case OP_LOG: case OP_SIN: {
+            case OP_SQRT: case OP_EXP: case OP_LOG: case OP_SIN: case OP_COS: {
                 auto f32 = [&](float x) -> float {
                     switch (op) {
                         case OP_SQRT: return o_sqrt(x);
                         case OP_EXP: return expf(x);
                         case OP_LOG: return logf(x);
+                        case OP_COS: return cosf(x);
                         default: return sinf(x);
                     }
                 };
@@ -1355,6 +1356,7 @@ int oracle_unary(int op, const OrArr* a, OrArr* out, int* fpe) {
                         case OP_SQRT: return o_sqrt(x);
                         case OP_EXP: return exp(x);
                         case OP_LOG: return log(x);
+                        case OP_COS: return cos(x);
                         default: return sin(x);
                     }
                 };

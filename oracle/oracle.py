@@ -40,7 +40,7 @@ OPS = {
     "floor_divide": 18, "left_shift": 19, "right_shift": 20,
     "remainder": 32, "fmod": 33,
     "negative": 64, "absolute": 65, "invert": 66, "logical_not": 67,
-    "sqrt": 80, "exp": 81, "log": 82, "sin": 83,
+    "sqrt": 80, "exp": 81, "log": 82, "sin": 83, "cos": 84,
 }
 FPE_NAMES = {0: None, 1: "divide", 2: "over", 4: "under", 8: "invalid"}
 STATUS = {1: "broadcast", 2: "type", 3: "value", 4: "no_loop", 5: "axis", 9: "unsupported"}
@@ -474,11 +474,11 @@ def at(op: str, target: np.ndarray, indices, values=None):
       that dtype cast back at the end;
     * unary: logical_not in bool, stored back as 0/1; negative / absolute /
       invert only where they keep the dtype (else TypeError "'.at' would
-      change dtype ..."); sqrt / exp / log / sin in their float loop dtype,
+      change dtype ..."); sqrt / exp / log / sin / cos in their float loop dtype,
       cast back after every application."""
     dt = target.dtype
     if values is None:
-        math = op in ("sqrt", "exp", "log", "sin")
+        math = op in ("sqrt", "exp", "log", "sin", "cos")
         if math:
             unary_out_dtype(op, dt)          # checked before the indices
         rows = at_rows(target.shape, indices)

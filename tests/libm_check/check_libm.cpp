@@ -1,7 +1,7 @@
-// Host check of the product's exp/log/sin (anionpy_b200/csrc/ionp_libm.cuh,
+// Host check of the product's exp/log/sin/cos (anionpy_b200/csrc/ionp_libm.cuh,
 // compiled here for the CPU) against the host C library, the oracle of the
 // transcendental ufuncs. Every result must have the same bits, NaNs included.
-//   check_libm f32 <stride>   every stride-th float32 bit pattern, exp/log/sin
+//   check_libm f32 <stride>   every stride-th float32 bit pattern, exp/log/sin/cos
 //   check_libm f64 <count>    count seeded float64 arguments per function,
 //                             drawn from ranges that reach every code path
 // Prints one line per function: "<name> n=<checked> diff=<mismatches>".
@@ -58,26 +58,26 @@ int main(int argc, char** argv) {
     const uint64_t arg = argc > 2 ? strtoull(argv[2], nullptr, 10) : 1;
     if (f32) {
         const uint64_t stride = arg ? arg : 1;
-        const char* names[3] = {"exp32", "log32", "sin32"};
-        for (int fn = 0; fn < 3; fn++)
+        const char* names[4] = {"exp32", "log32", "sin32", "cos32"};
+        for (int fn = 0; fn < 4; fn++)
             run(names[fn], 0, nt, [&](int t, int T, uint64_t* d, uint64_t* c) {
                 for (uint64_t u = (uint64_t)t * stride; u <= 0xFFFFFFFFull; u += (uint64_t)T * stride) {
                     const float x = ffrom((uint32_t)u);
-                    const float m = fn == 0 ? exp32(x) : fn == 1 ? log32(x) : sin32(x);
-                    const float g = fn == 0 ? expf(x) : fn == 1 ? logf(x) : sinf(x);
+                    const float m = fn == 0 ? exp32(x) : fn == 1 ? log32(x) : fn == 2 ? sin32(x) : cos32(x);
+                    const float g = fn == 0 ? expf(x) : fn == 1 ? logf(x) : fn == 2 ? sinf(x) : cosf(x);
                     ++*c;
                     if (fbits(m) != fbits(g)) ++*d;
                 }
             });
     } else {
-        const char* names[3] = {"exp64", "log64", "sin64"};
-        for (int fn = 0; fn < 3; fn++)
+        const char* names[4] = {"exp64", "log64", "sin64", "cos64"};
+        for (int fn = 0; fn < 4; fn++)
             run(names[fn], 0, nt, [&](int t, int T, uint64_t* d, uint64_t* c) {
                 uint64_t st[2] = {0x9E3779B97F4A7C15ull * (uint64_t)(t + 1 + 64 * fn), 0xD1B54A32D192ED03ull};
                 for (uint64_t i = (uint64_t)t; i < arg; i += (uint64_t)T) {
-                    const double x = draw(next(st), (int)(i % 6), fn);
-                    const double m = fn == 0 ? exp64(x) : fn == 1 ? log64(x) : sin64(x);
-                    const double g = fn == 0 ? exp(x) : fn == 1 ? log(x) : sin(x);
+                    const double x = draw(next(st), (int)(i % 6), fn < 3 ? fn : 2);   // cos: sin's ranges
+                    const double m = fn == 0 ? exp64(x) : fn == 1 ? log64(x) : fn == 2 ? sin64(x) : cos64(x);
+                    const double g = fn == 0 ? exp(x) : fn == 1 ? log(x) : fn == 2 ? sin(x) : cos(x);
                     ++*c;
                     if (dbits(m) != dbits(g)) ++*d;
                 }

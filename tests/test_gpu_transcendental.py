@@ -1,8 +1,9 @@
-"""GPU exp / log / sin: identical bits to the oracle, the host C library that
-the reference's f32::exp/ln/sin and f64::exp/ln/sin call on Linux
-(ionp-core/src/ufunc.rs:4237-4367). The reference records 0 ULP for exp and
-log and for float64 sin (tests/differential/ufunc_registry.py); float32 sin
-is held to the same 0 ULP here. NaN results must match bit for bit too."""
+"""GPU exp / log / sin / cos: identical bits to the oracle, the host C library
+that the reference's f32::exp/ln/sin/cos and f64::exp/ln/sin/cos call on
+Linux (ionp-core/src/ufunc.rs:4237-4367). The reference records 0 ULP for exp
+and log and for float64 sin and cos (tests/differential/ufunc_registry.py);
+float32 sin and cos are held to the same 0 ULP here. NaN results must match
+bit for bit too."""
 import numpy as np
 import pytest
 
@@ -27,20 +28,20 @@ def f32_patterns(stride, offset):
     return np.arange(offset, 1 << 32, stride, dtype=np.uint64).astype(np.uint32).view(np.float32)
 
 
-@pytest.mark.parametrize("fn", ["exp", "log", "sin"])
+@pytest.mark.parametrize("fn", ["exp", "log", "sin", "cos"])
 def test_float32_bit_patterns(fn):
     check(fn, f32_patterns(251, 17), "float32 every 251st bit pattern")
 
 
-@pytest.mark.parametrize("fn", ["exp", "log", "sin"])
+@pytest.mark.parametrize("fn", ["exp", "log", "sin", "cos"])
 @pytest.mark.parametrize("dt", [np.float32, np.float64], ids=lambda d: np.dtype(d).name)
 def test_benchmark_distributions(fn, dt):
     """the distributions of the 2^28-element sweep: exp on U[-100, 100], log
-    on U(0, 1e6], sin on 10 N(0, 1)"""
+    on U(0, 1e6], sin (and cos) on 10 N(0, 1)"""
     rng = np.random.default_rng(11)
     n = 1 << 20
     x = {"exp": rng.uniform(-100, 100, n), "log": 1e6 * (1 - rng.random(n)),
-         "sin": 10 * rng.standard_normal(n)}[fn]
+         "sin": 10 * rng.standard_normal(n), "cos": 10 * rng.standard_normal(n)}[fn]
     with np.errstate(all="ignore"):
         x = np.concatenate([np.array(SPECIALS), x]).astype(dt)
     check(fn, x, f"{np.dtype(dt).name} sweep distribution")
@@ -49,8 +50,8 @@ def test_benchmark_distributions(fn, dt):
 def f64_classes(fn, n, seed):
     """float64 arguments reaching every path of the restated algorithms:
     any bit pattern, moderate exponents, exp's subnormal and overflow ends,
-    log near 1 and subnormals, sin in each reduction range, near multiples of
-    pi/2 and beyond 105414350"""
+    log near 1 and subnormals, sin and cos in each reduction range, near
+    multiples of pi/2 and beyond 105414350"""
     rng = np.random.default_rng(seed)
     u = rng.integers(0, 2 ** 63, n, dtype=np.int64).astype(np.uint64) * np.uint64(2) + rng.integers(0, 2, n).astype(np.uint64)
     parts = [u.view(np.float64)]
@@ -69,12 +70,12 @@ def f64_classes(fn, n, seed):
     return np.concatenate([np.array(SPECIALS)] + parts)
 
 
-@pytest.mark.parametrize("fn", ["exp", "log", "sin"])
+@pytest.mark.parametrize("fn", ["exp", "log", "sin", "cos"])
 def test_float64_all_paths(fn):
     check(fn, f64_classes(fn, 1 << 18, 5), "float64 path classes")
 
 
-@pytest.mark.parametrize("fn", ["exp", "log", "sin"])
+@pytest.mark.parametrize("fn", ["exp", "log", "sin", "cos"])
 def test_float16_and_int_promotion(fn):
     rng = np.random.default_rng(3)
     x16 = np.arange(1 << 16, dtype=np.uint32).astype(np.uint16).view(np.float16)   # every float16
@@ -99,7 +100,7 @@ def test_log_fpe():
             ap.log(ap.from_numpy(np.array([0.0, -1.0], np.float32)))
 
 
-@pytest.mark.parametrize("fn", ["exp", "log", "sin"])
+@pytest.mark.parametrize("fn", ["exp", "log", "sin", "cos"])
 @pytest.mark.parametrize("dt", [np.float32, np.float64], ids=lambda d: np.dtype(d).name)
 def test_strided_slices(fn, dt):
     """Step-2 and step-3 slices and a reversed view give the oracle's bits,

@@ -15,7 +15,7 @@ ap = pytest.importorskip("anionpy_b200")
 pytestmark = pytest.mark.gpu
 
 BIN_OPS = list(O.BINARY_AT_OPS)
-UN_OPS = ["negative", "absolute", "invert", "logical_not", "sqrt", "exp", "log", "sin"]
+UN_OPS = ["negative", "absolute", "invert", "logical_not", "sqrt", "exp", "log", "sin", "cos"]
 IDX = [0, 3, -1, 0, 2, 3, 3, 5]
 
 
