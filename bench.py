@@ -812,8 +812,19 @@ NCU_TRAFFIC_PER_BYTE = {"floor_divide/float64/transposed": 0.9800, "add/float32/
                         "floor_divide/int64/transposed": 0.9660}
 
 
+# The other 8-byte binaries on the step-2 slice run the same kernel
+# (k_bin_run) over the same access pattern as the measured step-2 division
+# cases (both operands every other element of a 2n base, output contiguous),
+# so their DRAM bytes per algorithmic byte are those cases' (1.611).
+STEP2_8B_BINARY_TRAFFIC = 1.611
+
+
 def traffic_of(case, alg_bytes):
     r = NCU_TRAFFIC_PER_BYTE.get(case)
+    if r is None:
+        op, dt, lay = (case.split("/") + ["", "", ""])[:3]
+        if lay == "step2" and dt in ("int64", "float64") and op not in UN_OPS:
+            r = STEP2_8B_BINARY_TRAFFIC
     return None if r is None else int(round(r * alg_bytes))
 
 
